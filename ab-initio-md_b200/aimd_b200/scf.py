@@ -1,0 +1,736 @@
+"""
+Restricted / unrestricted Hartree-Fock SCF on the GPU, with the reference's
+API and semantics (``aimd.qc.scf``, aimd/qc/scf.py:1-982):
+
+  SCFOptions, SCFResult, SCFSolver, run_scf, DIIS, orthogonalizer,
+  electron_counts, check_nuclear_separation, SCFConvergenceWarning
+
+Differences in method, not in results: the Fock build is integral-direct
+(no stored ERI tensor, so ``max_nao`` no longer limits the basis size), and
+every matrix of the iteration (S, h, X, D, F, DIIS history, eigenvectors)
+lives on the device in FP64. F_s = h + g sum J - K_s with g = 2 / nspin,
+E_el = 1/2 g sum_s tr D_s (h + F_s), orbital gradient X^T (F D S - S D F) X,
+Pulay DIIS anchored on the newest vector and solved by SVD, level shift and
+damping while the commutator exceeds ``stabilize_until``, aufbau occupation.
+Non-convergence returns the last iterate flagged, never raises.
+"""
+
+from __future__ import annotations
+
+import time
+import warnings
+from dataclasses import dataclass, field, fields, replace
+from typing import Any, Sequence
+
+import numpy as np
+import torch
+
+from . import integrals as I
+from .basis import BasisSet, build_basis
+from .elements import normalize_symbol
+
+LINDEP_THRESHOLD = 1e-7
+GWH_K = 1.75
+MIN_NUCLEAR_SEPARATION = 1e-5
+_GUESSES = ("sad", "core", "gwh")
+_ORTHO = ("auto", "symmetric", "canonical")
+_REFERENCES = {"rhf": "rhf", "restricted": "rhf", "uhf": "uhf", "unrestricted": "uhf"}
+_DEV = "cuda"
+
+
+class SCFConvergenceWarning(RuntimeWarning):
+    """Emitted by the direct API when an SCF stops at max_iter unconverged."""
+
+
+@dataclass(frozen=True)
+class SCFOptions:
+    """SCF settings; names, defaults and validation as aimd/qc/scf.py:185-247."""
+    conv_energy: float = 1e-10
+    conv_commutator: float = 1e-7
+    max_iter: int = 100
+    guess: str = "sad"
+    diis: bool = True
+    diis_space: int = 8
+    diis_restart: int = 12
+    level_shift: float = 0.0
+    damping: float = 0.0
+    stabilize_until: float = 1e-3
+    orthogonalization: str = "auto"
+    lindep_threshold: float = LINDEP_THRESHOLD
+    schwarz_threshold: float = I.DEFAULT_SCHWARZ
+    max_nao: int = I.MAX_NAO_ERI          # kept for compatibility; the direct build stores no tensor
+    warn_unconverged: bool = True
+    blas_threads: int | None = 1          # kept for compatibility; no host BLAS in the loop
+
+    def __post_init__(self) -> None:
+        if not (self.conv_energy > 0.0 and self.conv_commutator > 0.0):
+            raise ValueError("SCF convergence thresholds must be positive")
+        if self.max_iter < 1:
+            raise ValueError("max_iter must be >= 1")
+        if self.guess not in _GUESSES:
+            raise ValueError(f"unknown guess {self.guess!r}; use one of {_GUESSES}")
+        if self.diis_space < 2:
+            raise ValueError("diis_space must be >= 2")
+        if self.diis_restart < 0:
+            raise ValueError("diis_restart must be >= 0")
+        if self.level_shift < 0.0:
+            raise ValueError("level_shift must be >= 0")
+        if not 0.0 <= self.damping < 1.0:
+            raise ValueError("damping must be in [0, 1)")
+        if self.orthogonalization not in _ORTHO:
+            raise ValueError(f"unknown orthogonalization {self.orthogonalization!r}; use one of {_ORTHO}")
+        if not self.lindep_threshold > 0.0:
+            raise ValueError("lindep_threshold must be positive")
+        if self.blas_threads is not None and self.blas_threads < 1:
+            raise ValueError("blas_threads must be >= 1 or None")
+
+
+def electron_counts(nuclear_charge: int, charge: int, multiplicity: int, reference: str = "uhf") -> tuple[int, int]:
+    """(n_alpha, n_beta); ValueError for impossible combinations (aimd/qc/scf.py:250-281)."""
+    n = int(nuclear_charge) - int(charge)
+    mult = int(multiplicity)
+    if n <= 0:
+        raise ValueError(f"charge {charge} leaves {n} electrons; need at least one")
+    if mult < 1:
+        raise ValueError(f"multiplicity must be >= 1, got {mult}")
+    if (n + mult - 1) % 2:
+        raise ValueError(f"multiplicity {mult} is impossible with {n} electrons")
+    if mult - 1 > n:
+        raise ValueError(f"multiplicity {mult} needs at least {mult - 1} electrons, have {n}")
+    na, nb = (n + mult - 1) // 2, (n - mult + 1) // 2
+    ref = str(reference).strip().lower()
+    if ref not in _REFERENCES:
+        raise ValueError(f"unknown reference {reference!r}; use 'rhf' or 'uhf'")
+    if _REFERENCES[ref] == "rhf" and na != nb:
+        raise ValueError(f"RHF needs a closed-shell singlet; {n} electrons with multiplicity {mult} is open-shell")
+    return na, nb
+
+
+def check_nuclear_separation(positions, atomic_numbers) -> None:
+    """ValueError if two nuclei are closer than 1e-5 bohr (aimd/qc/scf.py:666-684)."""
+    x = np.asarray(positions, dtype=float).reshape(-1, 3)
+    z = np.asarray(atomic_numbers)
+    if len(x) < 2 or not np.all(np.isfinite(x)):
+        return
+    r = np.linalg.norm(x[:, None, :] - x[None, :, :], axis=-1)
+    i, j = np.triu_indices(len(x), k=1)
+    bad = (r[i, j] < MIN_NUCLEAR_SEPARATION) & (z[i] > 0) & (z[j] > 0)
+    if np.any(bad):
+        k = int(np.argmax(bad))
+        raise ValueError(f"atoms {i[k]} and {j[k]} are {r[i[k], j[k]]:.3g} bohr apart (coincident nuclei, "
+                         f"< {MIN_NUCLEAR_SEPARATION:g} bohr): the nuclear repulsion is infinite")
+
+
+def orthogonalizer(S: torch.Tensor, method: str = "auto", threshold: float = LINDEP_THRESHOLD):
+    """X with X^T S X = 1, removed combinations, smallest overlap eigenvalue (aimd/qc/scf.py:284-303)."""
+    if method not in _ORTHO:
+        raise ValueError(f"unknown orthogonalization {method!r}; use one of {_ORTHO}")
+    s, U = torch.linalg.eigh(S)
+    smin = float(s[0])
+    keep = s >= threshold
+    nkeep = int(keep.sum())
+    if method == "symmetric" or (method == "auto" and nkeep == len(s)):
+        if nkeep != len(s):
+            raise ValueError(f"overlap eigenvalue {smin:.3e} < lindep_threshold {threshold:.1e}: the basis is "
+                             "nearly linearly dependent; use canonical orthogonalization")
+        return (U * s.rsqrt()) @ U.T, 0, smin
+    if nkeep == 0:
+        raise ValueError("every overlap eigenvalue is below lindep_threshold")
+    return U[:, keep] * s[keep].rsqrt(), len(s) - nkeep, smin
+
+
+class DIIS:
+    """
+    Pulay DIIS over stacks (nspin, nmo, nmo) on the device (aimd/qc/scf.py:
+    516-568): min |e_m + sum_{i<m} c_i (e_i - e_m)|, solved as a minimum-norm
+    least-squares problem by QR of the difference vectors (device) and SVD of
+    the small triangular factor, with numpy's default singular-value cutoff
+    eps * max(rows, cols); coefficients above ``max_coefficient`` drop the
+    oldest vectors.
+    """
+
+    def __init__(self, space: int = 8, max_coefficient: float = 1e4) -> None:
+        self.space, self.max_coefficient = int(space), float(max_coefficient)
+        self.focks: list[torch.Tensor] = []
+        self.errors: list[torch.Tensor] = []
+
+    def __len__(self) -> int:
+        return len(self.focks)
+
+    def reset(self) -> None:
+        self.focks.clear()
+        self.errors.clear()
+
+    def push(self, fock: torch.Tensor, error: torch.Tensor) -> None:
+        self.focks.append(fock.clone())
+        self.errors.append(error.clone())
+        while len(self.focks) > self.space:
+            self.focks.pop(0)
+            self.errors.pop(0)
+
+    def coefficients(self) -> np.ndarray:
+        if len(self.errors) == 1:
+            return np.ones(1)
+        last = self.errors[-1].reshape(-1)
+        delta = torch.stack([e.reshape(-1) - last for e in self.errors[:-1]], dim=1)
+        Qm, Rm = torch.linalg.qr(delta)
+        rhs = (Qm.T @ (-last)).cpu().numpy()
+        R = Rm.cpu().numpy()
+        U, s, Vt = np.linalg.svd(R)
+        cut = np.finfo(float).eps * max(delta.shape) * (s[0] if s.size else 0.0)
+        inv = np.where(s > cut, 1.0 / np.where(s > cut, s, 1.0), 0.0)
+        x = Vt.T @ (inv * (U.T @ rhs))
+        return np.append(x, 1.0 - x.sum())
+
+    def extrapolate(self) -> torch.Tensor:
+        while len(self.focks) > 1:
+            c = self.coefficients()
+            if np.all(np.isfinite(c)) and np.abs(c).max() <= self.max_coefficient:
+                out = torch.zeros_like(self.focks[0])
+                for ci, Fi in zip(c, self.focks):
+                    out += float(ci) * Fi
+                return out
+            self.focks.pop(0)
+            self.errors.pop(0)
+        return self.focks[-1].clone()
+
+
+@dataclass(frozen=True, eq=False)
+class SCFIntegrals:
+    """S, h = T + V, X and E_nuc at one geometry (device tensors)."""
+    basis: BasisSet
+    S: torch.Tensor
+    H: torch.Tensor
+    X: torch.Tensor
+    n_removed: int
+    min_overlap_eigenvalue: float
+    nuclear_repulsion: float
+    M: torch.Tensor              # dipole integrals about the origin, (3, n, n)
+
+    @property
+    def nao(self) -> int:
+        return self.basis.nao
+
+    @property
+    def nmo(self) -> int:
+        return int(self.X.shape[1])
+
+
+def build_integrals(basis: BasisSet, options: SCFOptions | None = None) -> SCFIntegrals:
+    opt = options or SCFOptions()
+    S, T, M, V = I.one_electron_device(basis)
+    X, n_removed, smin = orthogonalizer(S, opt.orthogonalization, opt.lindep_threshold)
+    enuc = I.nuclear_repulsion_energy(basis.nuclear_charges, basis.positions)
+    return SCFIntegrals(basis, S, T + V, X, n_removed, smin, enuc, M)
+
+
+# ---------------------------------------------------------------- guesses
+
+_MADELUNG = sorted(((n, l) for n in range(1, 8) for l in range(n)), key=lambda t: (t[0] + t[1], t[0]))
+
+
+def ground_state_l_counts(Z: int) -> list[int]:
+    """Electrons per l of a neutral atom in Madelung order (aimd/qc/scf.py:365-380)."""
+    counts, left = [0, 0, 0, 0], int(Z)
+    for _n, l in _MADELUNG:
+        if left <= 0:
+            break
+        k = min(left, 2 * (2 * l + 1))
+        counts[l] += k
+        left -= k
+    return counts
+
+
+def _atomic_occupations(eps: np.ndarray, l_counts: Sequence[int], tol: float = 1e-6) -> np.ndarray:
+    """Spherical fractional occupations by degenerate groups (aimd/qc/scf.py:396-427)."""
+    groups, i = [], 0
+    while i < len(eps):
+        j = i + 1
+        while j < len(eps) and eps[j] - eps[j - 1] < tol:
+            j += 1
+        groups.append((i, j))
+        i = j
+    occ = np.zeros(len(eps))
+    left = list(l_counts) + [0] * (5 - len(l_counts))
+    ok = True
+    for i, j in groups:
+        g = j - i
+        if g % 2 == 0 or g > 9:
+            ok = False
+            break
+        l = (g - 1) // 2
+        k = min(left[l], 2 * g)
+        occ[i:j] = k / g
+        left[l] -= k
+    if ok and not any(left):
+        return occ
+    occ[:] = 0.0
+    n = float(sum(l_counts))
+    for i, j in groups:
+        k = min(n, 2.0 * (j - i))
+        occ[i:j] = k / (j - i)
+        n -= k
+    return occ
+
+
+_ATOMIC_CACHE: dict[tuple, tuple[np.ndarray, float, bool]] = {}
+
+
+def atom_basis(basis: BasisSet, atom: int) -> BasisSet:
+    """The shells of one atom as a one-atom basis at the origin."""
+    sh = np.flatnonzero(basis.shell_atom == atom)
+    k0 = [basis.shell_prim[s] for s in sh]
+    k1 = [basis.shell_prim[s + 1] for s in sh]
+    prim = np.concatenate([np.arange(a, b) for a, b in zip(k0, k1)]) if len(sh) else np.zeros(0, int)
+    shell_prim = np.concatenate([[0], np.cumsum([b - a for a, b in zip(k0, k1)])])
+    return BasisSet(basis.name, [basis.symbols[atom]], np.zeros((1, 3)), np.zeros(len(sh), dtype=np.int64),
+                    basis.shell_l[sh], shell_prim, basis.prim_exp[prim], basis.prim_coef[prim])
+
+
+def atomic_hf(ab: BasisSet, max_iter: int = 200) -> tuple[np.ndarray, float, bool]:
+    """
+    Spherically averaged, fractional-occupation, spin-restricted HF of a
+    neutral atom in its molecular basis (aimd/qc/scf.py:433-482), on the
+    device; H gets its exact one-electron ground state. Cached per element
+    and shell data.
+    """
+    key = (int(ab.atomic_numbers[0]), ab.shell_l.tobytes(), ab.shell_prim.tobytes(), ab.prim_exp.tobytes(),
+           ab.prim_coef.tobytes())
+    hit = _ATOMIC_CACHE.get(key)
+    if hit is not None:
+        return hit[0].copy(), hit[1], hit[2]
+    Z = int(ab.atomic_numbers[0])
+    lc = ground_state_l_counts(Z)
+    S, T, _, V = I.one_electron_device(ab)
+    H = T + V
+    X, _, _ = orthogonalizer(S, "canonical", LINDEP_THRESHOLD)
+    if Z == 1:
+        eps, Cp = torch.linalg.eigh(X.T @ H @ X)
+        c = X @ Cp[:, 0]
+        res = (torch.outer(c, c).cpu().numpy(), float(eps[0]), True)
+        _ATOMIC_CACHE[key] = res
+        return res[0].copy(), res[1], True
+
+    def density(Fo: torch.Tensor) -> torch.Tensor:
+        eps, Cp = torch.linalg.eigh(Fo)
+        C = X @ Cp
+        occ = torch.as_tensor(_atomic_occupations(eps.cpu().numpy(), lc), device=C.device)
+        return (C * occ) @ C.T
+
+    D = density(X.T @ H @ X)
+    diis = DIIS(8)
+    e_old = np.inf
+    converged = False
+    e = 0.0
+    for _ in range(max_iter):
+        J, K = I.jk_device(ab, D[None].contiguous(), symmetric=True)
+        F = H + J[0] - 0.5 * K[0]
+        F = 0.5 * (F + F.T)
+        e = 0.5 * float(torch.sum(D * (H + F)))
+        err = X.T @ (F @ D @ S - S @ D @ F) @ X
+        if abs(e - e_old) < 1e-11 and float(err.abs().max()) < 1e-8:
+            converged = True
+            break
+        e_old = e
+        diis.push((X.T @ F @ X)[None], err[None])
+        D = density(diis.extrapolate()[0])
+    res = ((0.5 * (D + D.T)).cpu().numpy(), e, converged)
+    _ATOMIC_CACHE[key] = res
+    return res[0].copy(), e, converged
+
+
+def sad_density(basis: BasisSet) -> np.ndarray:
+    """Superposition of atomic densities (total density, (nao, nao))."""
+    P = np.zeros((basis.nao, basis.nao))
+    for a in range(basis.natm):
+        i, j = basis.atom_ao[a]
+        if j > i:
+            P[i:j, i:j] = atomic_hf(atom_basis(basis, a))[0]
+    return P
+
+
+def _occupied_density(F: torch.Tensor, X: torch.Tensor, nocc: int) -> torch.Tensor:
+    _, Cp = torch.linalg.eigh(X.T @ F @ X)
+    C = X @ Cp[:, :nocc]
+    return C @ C.T
+
+
+# ---------------------------------------------------------------- result
+
+@dataclass(eq=False)
+class SCFResult:
+    """SCF state at one geometry; fields as aimd/qc/scf.py:573-656 (numpy arrays)."""
+    reference: str
+    converged: bool
+    iterations: int
+    energy: float
+    electronic_energy: float
+    nuclear_repulsion: float
+    mo_energy: np.ndarray
+    mo_coeff: np.ndarray
+    mo_occ: np.ndarray
+    spin_densities: np.ndarray
+    fock: np.ndarray
+    energy_weighted_density: np.ndarray
+    mulliken_charges: np.ndarray
+    dipole: np.ndarray
+    s2: float
+    n_alpha: int
+    n_beta: int
+    energy_change: float
+    commutator_norm: float
+    basis: BasisSet
+    n_removed: int = 0
+    guess: str = ""
+    diis_restarts: int = 0
+    history: list[dict[str, float]] = field(default_factory=list)
+    timings: dict[str, float] = field(default_factory=dict)
+    device: dict[str, Any] = field(default_factory=dict, repr=False)   # device copies (Ds, F, W)
+
+    @property
+    def unrestricted(self) -> bool:
+        return self.reference == "uhf"
+
+    @property
+    def density(self) -> np.ndarray:
+        return self.spin_densities[0] + self.spin_densities[1]
+
+    @property
+    def density_alpha(self) -> np.ndarray:
+        return self.spin_densities[0]
+
+    @property
+    def density_beta(self) -> np.ndarray:
+        return self.spin_densities[1]
+
+    @property
+    def spin_density(self) -> np.ndarray:
+        return self.spin_densities[0] - self.spin_densities[1]
+
+    @property
+    def guess_density(self) -> np.ndarray:
+        return self.spin_densities.copy() if self.unrestricted else self.density
+
+    @property
+    def nmo(self) -> int:
+        return int(self.mo_coeff.shape[-1])
+
+    @property
+    def s2_exact(self) -> float:
+        sz = 0.5 * (self.n_alpha - self.n_beta)
+        return sz * (sz + 1.0)
+
+    def coulomb_exchange_densities(self):
+        if self.unrestricted:
+            return self.density, [self.density_alpha, self.density_beta], 1.0
+        P = self.density
+        return P, [P], 0.5
+
+    def __repr__(self) -> str:
+        flag = "converged" if self.converged else "NOT CONVERGED"
+        return (f"SCFResult({self.reference.upper()}/{self.basis.name}, E = {self.energy:.10f} Eh, "
+                f"{self.iterations} iterations, {flag})")
+
+
+# ---------------------------------------------------------------- solver
+
+class SCFSolver:
+    """
+    Reusable RHF/UHF solver for one molecule (aimd/qc/scf.py:687-965): the
+    basis is parsed once and its device engine reused for every geometry.
+    """
+
+    def __init__(self, symbols: Sequence[str], basis: str | BasisSet = "sto-3g", charge: int = 0,
+                 multiplicity: int = 1, reference: str | None = None, options: SCFOptions | None = None,
+                 **overrides: Any) -> None:
+        opt = options or SCFOptions()
+        if overrides:
+            known = {f.name for f in fields(SCFOptions)}
+            bad = sorted(set(overrides) - known)
+            if bad:
+                raise TypeError(f"unknown SCF option(s): {', '.join(bad)}")
+            opt = replace(opt, **overrides)
+        self.options = opt
+        n = len(symbols)
+        if isinstance(basis, BasisSet):
+            if [normalize_symbol(s) for s in symbols] != basis.symbols:
+                raise ValueError("symbols do not match the atoms of the given BasisSet")
+            self.basis = basis
+        else:
+            self.basis = build_basis(symbols, np.zeros((n, 3)), basis)
+        self.symbols = list(self.basis.symbols)
+        self.charge = int(charge)
+        self.multiplicity = int(multiplicity)
+        if reference is None:
+            ref = "rhf" if self.multiplicity == 1 else "uhf"
+        else:
+            key = str(reference).strip().lower()
+            if key not in _REFERENCES:
+                raise ValueError(f"unknown reference {reference!r}; use 'rhf' or 'uhf'")
+            ref = _REFERENCES[key]
+        self.reference = ref
+        self.n_alpha, self.n_beta = electron_counts(int(self.basis.atomic_numbers.sum()), self.charge,
+                                                    self.multiplicity, ref)
+        if self.n_alpha > self.basis.nao:
+            raise ValueError(f"{self.n_alpha} alpha electrons do not fit in {self.basis.nao} AOs")
+        self._ints: SCFIntegrals | None = None
+        self._ints_positions: np.ndarray | None = None
+        self._ints_options: SCFOptions | None = None
+        self._sad: np.ndarray | None = None
+
+    @property
+    def unrestricted(self) -> bool:
+        return self.reference == "uhf"
+
+    @property
+    def nao(self) -> int:
+        return self.basis.nao
+
+    @property
+    def nelectron(self) -> int:
+        return self.n_alpha + self.n_beta
+
+    @property
+    def density_shape(self) -> tuple[int, ...]:
+        n = self.nao
+        return (2, n, n) if self.unrestricted else (n, n)
+
+    def integrals(self, positions: np.ndarray) -> SCFIntegrals:
+        x = np.array(positions, dtype=float).reshape(-1, 3)
+        if x.shape[0] != self.basis.natm:
+            raise ValueError(f"expected {self.basis.natm} positions, got {x.shape[0]}")
+        if not np.all(np.isfinite(x)):
+            raise ValueError("atomic positions must be finite (got NaN or inf)")
+        check_nuclear_separation(x, self.basis.atomic_numbers)
+        if (self._ints is None or self._ints_options is not self.options
+                or not np.array_equal(x, self._ints_positions)):
+            self._ints = None
+            self._ints = build_integrals(self.basis.with_positions(x), self.options)
+            self._ints_positions = x
+            self._ints_options = self.options
+        return self._ints
+
+    def clear_cache(self) -> None:
+        self._ints = None
+        self._ints_positions = None
+
+    def _nocc(self) -> tuple[int, ...]:
+        return (self.n_alpha,) if not self.unrestricted else (self.n_alpha, self.n_beta)
+
+    def initial_spin_densities(self, ints_: SCFIntegrals, guess: Any) -> tuple[torch.Tensor, str]:
+        """(nspin, nao, nao) starting spin densities on the device and a label."""
+        nspin = 2 if self.unrestricted else 1
+        n = self.nao
+        if isinstance(guess, SCFResult):
+            if guess.basis.nao != n:
+                raise ValueError("guess SCFResult has a different basis")
+            D = guess.spin_densities
+            Ds = D[:nspin].copy() if self.unrestricted else 0.5 * (D[0] + D[1])[None]
+            return torch.as_tensor(Ds, device=_DEV), "result"
+        if guess is None:
+            guess = self.options.guess
+        if isinstance(guess, str):
+            kind = guess.strip().lower()
+            if kind == "sad":
+                if self._sad is None:
+                    self._sad = sad_density(self.basis)
+                Ds = torch.as_tensor(np.repeat(0.5 * self._sad[None], nspin, axis=0), device=_DEV)
+            elif kind in ("core", "gwh"):
+                if kind == "core":
+                    F = ints_.H
+                else:
+                    h = torch.diagonal(ints_.H)
+                    F = 0.5 * GWH_K * ints_.S * (h[:, None] + h[None, :])
+                    F.fill_diagonal_(0.0)
+                    F = F + torch.diag(h)
+                Ds = torch.stack([_occupied_density(F, ints_.X, k) for k in self._nocc()])
+            else:
+                raise ValueError(f"unknown guess {guess!r}; use one of {_GUESSES} or a density")
+            return Ds, kind
+        D = np.array(guess, dtype=float)
+        if D.shape == (n, n):
+            Ds = np.repeat(0.5 * D[None], nspin, axis=0)
+        elif D.shape == (2, n, n):
+            Ds = D.copy() if self.unrestricted else 0.5 * (D[0] + D[1])[None]
+        else:
+            raise ValueError(f"density guess has shape {D.shape}; expected {self.density_shape} "
+                             f"({self.reference.upper()}) or {(n, n) if self.unrestricted else (2, n, n)}")
+        if not np.all(np.isfinite(Ds)):
+            raise ValueError("density guess contains non-finite values")
+        return torch.as_tensor(0.5 * (Ds + Ds.transpose(0, 2, 1)), device=_DEV), "density"
+
+    def run(self, positions: np.ndarray, guess: Any = None) -> SCFResult:
+        return self._run(positions, guess, stacklevel=3)
+
+    def _run(self, positions: np.ndarray, guess: Any, stacklevel: int) -> SCFResult:
+        t0 = time.perf_counter()
+        Ik = self.integrals(positions)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        Ds, label = self.initial_spin_densities(Ik, guess)
+        t2 = time.perf_counter()
+        if Ik.nmo < self.n_alpha:
+            raise ValueError(f"{self.n_alpha} alpha electrons do not fit in {Ik.nmo} linearly independent orbitals")
+        state = self._iterate(Ik, Ds)
+        torch.cuda.synchronize()
+        t3 = time.perf_counter()
+        res = self._result(Ik, state, label)
+        res.timings = {"integrals": t1 - t0, "guess": t2 - t1, "iterations": t3 - t2,
+                       "total": time.perf_counter() - t0}
+        if not res.converged and self.options.warn_unconverged:
+            warnings.warn(f"SCF not converged after {res.iterations} iterations (dE = {res.energy_change:.2e} Eh, "
+                          f"commutator {res.commutator_norm:.2e}); returning the last iterate flagged "
+                          "converged=False", SCFConvergenceWarning, stacklevel=stacklevel)
+        return res
+
+    def _fock(self, Ik: SCFIntegrals, Ds: torch.Tensor) -> torch.Tensor:
+        g = 2.0 / Ds.shape[0]
+        J, K = I.jk_device(Ik.basis, Ds.contiguous(), self.options.schwarz_threshold, symmetric=True)
+        F = Ik.H + g * J.sum(dim=0) - K
+        return 0.5 * (F + F.transpose(1, 2))
+
+    def _iterate(self, Ik: SCFIntegrals, Ds: torch.Tensor) -> dict[str, Any]:
+        opt = self.options
+        nspin = Ds.shape[0]
+        g = 2.0 / nspin
+        nocc = self._nocc()
+        S, H, X = Ik.S, Ik.H, Ik.X
+        XtS = X.T @ S
+        diis = DIIS(opt.diis_space) if opt.diis else None
+        e_prev = np.nan
+        best = np.inf
+        since_best = 0
+        restarts = 0
+        history: list[dict[str, float]] = []
+        converged = False
+        eye = torch.eye(Ik.nmo, dtype=torch.float64, device=Ds.device)
+        for it in range(1, opt.max_iter + 1):
+            F = self._fock(Ik, Ds)
+            e_t = 0.5 * g * torch.sum(Ds * (H[None] + F))
+            FDS = F @ Ds @ S
+            err = X.T @ (FDS - FDS.transpose(1, 2)) @ X
+            e_el, err_norm = (float(v) for v in torch.stack([e_t, err.abs().max()]).cpu())
+            de = e_el - e_prev
+            history.append({"energy": e_el + Ik.nuclear_repulsion, "energy_change": de, "commutator": err_norm,
+                            "diis": len(diis) if diis else 0})
+            if abs(de) < opt.conv_energy and err_norm < opt.conv_commutator:
+                converged = True
+                break
+            if it == opt.max_iter:
+                break
+            Fo = X.T @ F @ X
+            if diis is not None:
+                if err_norm < best:
+                    best, since_best = err_norm, 0
+                else:
+                    since_best += 1
+                if opt.diis_restart and since_best >= opt.diis_restart:
+                    diis.reset()
+                    restarts += 1
+                    best, since_best = err_norm, 0
+                diis.push(Fo, err)
+                Fo = diis.extrapolate()
+            stabilize = err_norm > opt.stabilize_until
+            if stabilize and opt.level_shift > 0.0:
+                Do = XtS @ Ds @ XtS.T
+                Fo = Fo + opt.level_shift * (eye - Do)
+            Dn = torch.empty_like(Ds)
+            for s in range(nspin):
+                _, Cp = torch.linalg.eigh(Fo[s])
+                C = X @ Cp[:, :nocc[s]]
+                Dn[s] = C @ C.T
+            if stabilize and opt.damping > 0.0:
+                Dn = (1.0 - opt.damping) * Dn + opt.damping * Ds
+            Ds = Dn
+            e_prev = e_el
+        return {"Ds": Ds, "F": F, "e_el": e_el, "de": de, "err": err_norm, "it": it, "converged": converged,
+                "history": history, "restarts": restarts}
+
+    def _result(self, Ik: SCFIntegrals, st: dict[str, Any], label: str) -> SCFResult:
+        basis = Ik.basis
+        Ds, F = st["Ds"], st["F"]
+        nspin = Ds.shape[0]
+        g = 2.0 / nspin
+        nocc = self._nocc()
+        X, S = Ik.X, Ik.S
+        eps_l, C_l, occ_l = [], [], []
+        W = torch.zeros_like(S)
+        for s in range(nspin):
+            e_s, Cp = torch.linalg.eigh(X.T @ F[s] @ X)
+            Cs = X @ Cp
+            occ = torch.zeros(Ik.nmo, dtype=torch.float64, device=S.device)
+            occ[:nocc[s]] = g
+            Co = Cs[:, :nocc[s]]
+            W += g * (Co * e_s[:nocc[s]]) @ Co.T
+            eps_l.append(e_s)
+            C_l.append(Cs)
+            occ_l.append(occ)
+        spin = torch.stack([Ds[0], Ds[-1]])
+        P = spin[0] + spin[1]
+        q = torch.as_tensor(basis.nuclear_charges.copy(), device=S.device)
+        q = q.index_add(0, torch.as_tensor(basis.ao_atom, device=S.device), -torch.diagonal(P @ S))
+        dip = -torch.einsum("xmn,mn->x", Ik.M, P)
+        sz = 0.5 * (self.n_alpha - self.n_beta)
+        s2 = sz * (sz + 1.0) + self.n_beta - float(torch.sum((spin[0] @ S) * (spin[1] @ S).T)) if nspin == 2 else 0.0
+        eps = torch.stack(eps_l)
+        C = torch.stack(C_l)
+        occ = torch.stack(occ_l)
+        Fo = F
+        if nspin == 1:
+            eps, C, occ, Fo = eps[0], C[0], occ[0], F[0]
+        dip_np = dip.cpu().numpy() + I.nuclear_dipole(basis.nuclear_charges, basis.positions)
+        return SCFResult(
+            reference=self.reference, converged=st["converged"], iterations=st["it"],
+            energy=st["e_el"] + Ik.nuclear_repulsion, electronic_energy=st["e_el"],
+            nuclear_repulsion=Ik.nuclear_repulsion, mo_energy=eps.cpu().numpy(), mo_coeff=C.cpu().numpy(),
+            mo_occ=occ.cpu().numpy(), spin_densities=spin.cpu().numpy(), fock=Fo.cpu().numpy(),
+            energy_weighted_density=(0.5 * (W + W.T)).cpu().numpy(), mulliken_charges=q.cpu().numpy(),
+            dipole=dip_np, s2=float(s2), n_alpha=self.n_alpha, n_beta=self.n_beta,
+            energy_change=float(st["de"]), commutator_norm=st["err"], basis=basis, n_removed=Ik.n_removed,
+            guess=label, diis_restarts=st["restarts"], history=st["history"],
+            device={"spin": spin, "F": F, "S": S})
+
+
+@dataclass(eq=False)
+class DeviceSCFState:
+    """SCF state kept on the device (no host copies): the fast path of MD loops."""
+    basis: BasisSet
+    spin: torch.Tensor            # (2, n, n) spin densities [alpha, beta]
+    fock: torch.Tensor            # (nspin, n, n)
+    energy: float
+    electronic_energy: float
+    nuclear_repulsion: float
+    converged: bool
+    iterations: int
+    unrestricted: bool
+    dipole_ints: torch.Tensor     # (3, n, n) about the origin
+
+
+def run_device(solver: "SCFSolver", positions: np.ndarray, guess: torch.Tensor | None = None) -> DeviceSCFState:
+    """
+    One SCF at ``positions`` starting from a device density ``guess``
+    (protocol shape: (n, n) RHF total density, (2, n, n) UHF), or from the
+    solver's initial guess when None. Returns device tensors only.
+    """
+    Ik = solver.integrals(positions)
+    nspin = 2 if solver.unrestricted else 1
+    if guess is None:
+        Ds, _ = solver.initial_spin_densities(Ik, None)
+    elif guess.dim() == 2:
+        Ds = (0.5 * guess)[None].expand(nspin, -1, -1).contiguous()
+    else:
+        Ds = guess.contiguous() if nspin == 2 else (0.5 * (guess[0] + guess[1]))[None].contiguous()
+    Ds = 0.5 * (Ds + Ds.transpose(1, 2))
+    st = solver._iterate(Ik, Ds)
+    spin = torch.stack([st["Ds"][0], st["Ds"][-1]])
+    return DeviceSCFState(Ik.basis, spin, st["F"], st["e_el"] + Ik.nuclear_repulsion, st["e_el"],
+                          Ik.nuclear_repulsion, st["converged"], st["it"], solver.unrestricted, Ik.M)
+
+
+def run_scf(symbols: Sequence[str], positions: np.ndarray, basis: str | BasisSet = "sto-3g", charge: int = 0,
+            multiplicity: int = 1, reference: str | None = None, guess: Any = None,
+            options: SCFOptions | None = None, **overrides: Any) -> SCFResult:
+    """One-shot SCF: SCFSolver(...).run(positions, guess)."""
+    solver = SCFSolver(symbols, basis, charge=charge, multiplicity=multiplicity, reference=reference,
+                       options=options, **overrides)
+    return solver._run(positions, guess, stacklevel=3)

@@ -1,0 +1,186 @@
+// Device building blocks of the McMurchie-Davidson integrals (sm_100a).
+//
+// Boys function F_n(x): grid table (step 0.1) + Taylor series about the
+// nearest grid point for x < 40, asymptotic F_0 and upward recursion above
+// (Helgaker, Jorgensen & Olsen 2000, sec. 9.8.2; the reference's
+// aimd/qc/boys.py:88-114). Hermite expansion coefficients E^{ij}_t by the
+// Obara-Saika-type recursion of McMurchie & Davidson (aimd/qc/hermite.py:110),
+// Hermite Coulomb integrals R_tuv by the level recursion, evaluated in place
+// (aimd/qc/hermite.py:145).
+//
+// Everything is templated on the angular momenta of a quartet class, so the
+// work arrays have compile-time sizes and small classes live in registers.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace hf {
+
+constexpr int LMAX = 2;            // s, p, d: every built-in basis set
+constexpr int BOYS_COLS = 20;      // F_0..F_19 tabulated: orders up to 10 + 9 Taylor terms
+constexpr int BOYS_NGRID = 402;    // x_k = 0.1 k, k < 402
+constexpr int PPW = 16;            // doubles per primitive-pair record
+constexpr double PI = 3.14159265358979323846;
+constexpr double TWO_PI_2_5 = 34.98683665524972;   // 2 pi^(5/2)
+
+__host__ __device__ constexpr int nherm(int L) { return (L + 1) * (L + 2) * (L + 3) / 6; }
+__host__ __device__ constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
+// Contraction cap per block angular momentum: s blocks may carry 2
+// contractions (cc-pVDZ first-row atoms), others one. Larger general
+// contractions are split into blocks of at most this size on the host.
+__host__ __device__ constexpr int ncon_cap(int l) { return l == 0 ? 2 : 1; }
+// Linear Hermite index of (t, u, v): by total degree, then t descending,
+// then u descending (the reference's ordering, aimd/qc/hermite.py:73-80).
+__host__ __device__ constexpr int hidx(int t, int u, int v) {
+    return nherm(t + u + v - 1) + (u + v) * (u + v + 1) / 2 + v;
+}
+// Cartesian component i of angular momentum l in PySCF order.
+__host__ __device__ constexpr int cart_x(int l, int i) {
+    int n = 0;
+    for (int lx = l; lx >= 0; --lx)
+        for (int ly = l - lx; ly >= 0; --ly) { if (n == i) return lx; ++n; }
+    return 0;
+}
+__host__ __device__ constexpr int cart_y(int l, int i) {
+    int n = 0;
+    for (int lx = l; lx >= 0; --lx)
+        for (int ly = l - lx; ly >= 0; --ly) { if (n == i) return ly; ++n; }
+    return 0;
+}
+__host__ __device__ constexpr int cart_z(int l, int i) { return l - cart_x(l, i) - cart_y(l, i); }
+
+// pair class index <-> (la, lb), la >= lb
+__host__ __device__ constexpr int pcls(int la, int lb) { return la * (la + 1) / 2 + lb; }
+__host__ __device__ constexpr int cls_la(int c) { return c == 0 ? 0 : (c < 3 ? 1 : 2); }
+__host__ __device__ constexpr int cls_lb(int c) { return c - pcls(cls_la(c), 0); }
+constexpr int NCLS = 6;
+
+// Normalisation of Cartesian component (lx, ly, lz) relative to x^l:
+// sqrt((2l-1)!! / ((2lx-1)!! (2ly-1)!! (2lz-1)!!)).
+__host__ __device__ constexpr double dfact_odd(int n) { double r = 1.0; for (int k = n; k > 1; k -= 2) r *= k; return r; }
+__host__ __device__ inline double cart_norm(int lx, int ly, int lz) {
+    return sqrt(dfact_odd(2 * (lx + ly + lz) - 1) / (dfact_odd(2 * lx - 1) * dfact_odd(2 * ly - 1) * dfact_odd(2 * lz - 1)));
+}
+
+// ---------------------------------------------------------------- Boys
+
+// F_n(x) for one order n <= 10.
+__device__ __forceinline__ double boys_top(int n, double x, const double* __restrict__ tab) {
+    if (x < 40.0) {
+        const int k = static_cast<int>(x * 10.0 + 0.5);
+        const double dx = k * 0.1 - x;
+        const double* row = tab + k * BOYS_COLS + n;
+        // Horner form of sum_m F_{n+m}(x_k) dx^m / m!, m < 10
+        double acc = __ldg(row + 9);
+#pragma unroll
+        for (int m = 8; m >= 0; --m) acc = __ldg(row + m) + acc * dx * (1.0 / (m + 1));
+        return acc;
+    }
+    double f = 0.5 * sqrt(PI / x);
+    if (n > 0) {
+        const double ex = exp(-x), inv2x = 0.5 / x;
+        for (int m = 0; m < n; ++m) f = ((2 * m + 1) * f - ex) * inv2x;
+    }
+    return f;
+}
+
+// R_tuv(alpha, PQ) for all t+u+v <= L, in place: levels n = L..0, each level
+// overwriting the previous one in decreasing Hermite index (entries h only
+// read lower indices of the level above). R[0] of level n is (-2a)^n F_n.
+template <int L>
+__device__ __forceinline__ void hermite_r(double alpha, double X, double Y, double Z,
+                                          const double* __restrict__ tab, double (&R)[nherm(L)]) {
+    const double T = alpha * (X * X + Y * Y + Z * Z);
+    double f = boys_top(L, T, tab);
+    const double ex = (L > 0) ? exp(-T) : 0.0;
+    const double m2a = -2.0 * alpha;
+    double pw[L + 1];
+    pw[0] = 1.0;
+#pragma unroll
+    for (int n = 1; n <= L; ++n) pw[n] = pw[n - 1] * m2a;
+    R[0] = pw[L] * f;
+#pragma unroll
+    for (int n = L - 1; n >= 0; --n) {
+        f = (2.0 * T * f + ex) * (1.0 / (2 * n + 1));
+        // level n from level n+1; degrees d = L-n .. 1, decreasing index
+#pragma unroll
+        for (int d = L - n; d >= 1; --d) {
+#pragma unroll
+            for (int t = 0; t <= d; ++t) {
+#pragma unroll
+                for (int u = 0; u <= d - t; ++u) {
+                    const int v = d - t - u;
+                    double r;
+                    if (t > 0) {
+                        r = X * R[hidx(t - 1, u, v)];
+                        if (t > 1) r += (t - 1) * R[hidx(t - 2, u, v)];
+                    } else if (u > 0) {
+                        r = Y * R[hidx(t, u - 1, v)];
+                        if (u > 1) r += (u - 1) * R[hidx(t, u - 2, v)];
+                    } else {
+                        r = Z * R[hidx(t, u, v - 1)];
+                        if (v > 1) r += (v - 1) * R[hidx(t, u, v - 2)];
+                    }
+                    R[hidx(t, u, v)] = r;
+                }
+            }
+        }
+        R[0] = pw[n] * f;
+    }
+}
+
+// E^{ij}_t for i <= IM, j <= JM, t <= i + j, one direction: e[i][j][t].
+// pa = P - A, pb = P - B, oo2p = 1/(2p), e00 = E^{00}_0.
+template <int IM, int JM>
+__device__ __forceinline__ void hermite_e(double pa, double pb, double oo2p, double e00,
+                                          double (&e)[IM + 1][JM + 1][IM + JM + 1]) {
+#pragma unroll
+    for (int i = 0; i <= IM; ++i)
+#pragma unroll
+        for (int j = 0; j <= JM; ++j)
+#pragma unroll
+            for (int t = 0; t <= IM + JM; ++t) e[i][j][t] = 0.0;
+    e[0][0][0] = e00;
+#pragma unroll
+    for (int j = 1; j <= JM; ++j)
+#pragma unroll
+        for (int t = 0; t <= j; ++t) {
+            double v = pb * e[0][j - 1][t];
+            if (t + 1 <= j - 1) v += (t + 1) * e[0][j - 1][t + 1];
+            if (t > 0) v += oo2p * e[0][j - 1][t - 1];
+            e[0][j][t] = v;
+        }
+#pragma unroll
+    for (int i = 1; i <= IM; ++i)
+#pragma unroll
+        for (int j = 0; j <= JM; ++j)
+#pragma unroll
+            for (int t = 0; t <= i + j; ++t) {
+                double v = pa * e[i - 1][j][t];
+                if (t + 1 <= i - 1 + j) v += (t + 1) * e[i - 1][j][t + 1];
+                if (t > 0) v += oo2p * e[i - 1][j][t - 1];
+                e[i][j][t] = v;
+            }
+}
+
+// ---------------------------------------------------------------- data
+
+// Primitive-pair record (PPW doubles), pair oriented so that l_A >= l_B:
+//   0 a, 1 b, 2 K = exp(-mu |A-B|^2), 3..5 P, 6..8 P - A, 9..11 P - B,
+//   12..15 contraction products c_A[ca] c_B[cb] at index ca * ncon_B + cb
+struct PairView {
+    const int* pa_blk;      // [npair] block A (l_A >= l_B)
+    const int* pb_blk;      // [npair] block B
+    const int64_t* slot;    // [npair] first record of the pair
+    const int* npp;         // [npair] surviving primitive pairs
+    const double* rec;      // records
+};
+
+struct BlockView {
+    const int* atom;
+    const int* l;
+    const int* ncon;
+    const int* ao;          // AO of (contraction 0, component 0)
+};
+
+}  // namespace hf

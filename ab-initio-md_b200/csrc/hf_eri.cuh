@@ -1,0 +1,445 @@
+// Contracted block-quartet ERIs and their integral-direct J/K digestion.
+//
+// Work decomposition (one launch per bra pair class X):
+//   * one CTA per bra block pair P1 (class X, in Schwarz-sorted order);
+//   * the ket block pairs P2 of every class Y <= X that pass Q1 Q2 >= thr are
+//     a prefix of class Y's Q-sorted list (cut at P1's own position for
+//     Y == X, so each unordered pair of pairs is visited once);
+//   * one thread item = (ket pair P2, ket Cartesian component pair cd): it
+//     computes the column (ab|cd) for every bra row ab and every contraction
+//     combination, by McMurchie-Davidson: per primitive quartet R_tuv up to
+//     L = l_a+l_b+l_c+l_d, the ket Hermite->Cartesian step for its own cd,
+//     and after the ket primitive loop the bra step (the reference's
+//     _eri_block, aimd/qc/integrals.py:777-842, reorganised by column).
+// The bra pair's primitive E tables are staged once per CTA in shared
+// memory. Digestion: every exchange image of the 8-fold symmetry lands in a
+// row of the bra pair's functions, so K rows are accumulated in shared
+// memory and flushed once per CTA; J_ab accumulates in registers; only
+// J_cd goes straight to global memory.
+#pragma once
+#include "hf_device.cuh"
+
+namespace hf {
+
+template <int CX, int CY>
+struct QClass {
+    static constexpr int LA = cls_la(CX), LB = cls_lb(CX), LC = cls_la(CY), LD = cls_lb(CY);
+    static constexpr int LAB = LA + LB, LCD = LC + LD, L = LAB + LCD;
+    static constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+    static constexpr int NAB = NA * NB, NCD = NC * ND;
+    static constexpr int KA = ncon_cap(LA), KB = ncon_cap(LB), KC = ncon_cap(LC), KD = ncon_cap(LD);
+    static constexpr int KAB = KA * KB, KCD = KC * KD;
+    static constexpr int NROW = KAB * NAB;
+    static constexpr int NHB = nherm(LAB);
+};
+
+// Bra-side E tables with an extra +G in i and j (G = 1 for gradients).
+template <int LA, int LB, int G>
+struct BraE {
+    static constexpr int I = LA + 1 + G, J = LB + 1 + G, T = LA + LB + 1 + 2 * G;
+    static constexpr int SIZE = 3 * I * J * T;
+    __device__ static int at(int d, int i, int j, int t) { return ((d * I + i) * J + j) * T + t; }
+};
+
+// Shared-memory stage of one bra pair.
+struct BraStage {
+    int P1, A, B, nbp, aA, aB;
+    int nA, nB, oA, oB;
+    const double* rec;      // bra primitive records (global)
+    double* E;              // [nbp][BraE::SIZE] (shared)
+};
+
+// Fill stage->E for all bra primitives (block-cooperative).
+template <int LA, int LB, int G>
+__device__ __forceinline__ void stage_bra_e(const BraStage& st) {
+    using BE = BraE<LA, LB, G>;
+    for (int w = threadIdx.x; w < st.nbp * 3; w += blockDim.x) {
+        const int ib = w / 3, d = w % 3;
+        const double* b = st.rec + (size_t)ib * PPW;
+        const double p = b[0] + b[1];
+        double e[LA + 1 + G][LB + 1 + G][LA + LB + 1 + 2 * G];
+        hermite_e<LA + G, LB + G>(b[6 + d], b[9 + d], 0.5 / p, d == 0 ? b[2] : 1.0, e);
+        double* out = st.E + (size_t)ib * BE::SIZE;
+#pragma unroll
+        for (int i = 0; i < LA + 1 + G; ++i)
+#pragma unroll
+            for (int j = 0; j < LB + 1 + G; ++j)
+#pragma unroll
+                for (int t = 0; t < LA + LB + 1 + 2 * G; ++t) out[BE::at(d, i, j, t)] = e[i][j][t];
+    }
+}
+
+// v[r][kk] = (row r | cd, contraction kk) of the quartet (bra stage, ket pair
+// records rk with nkp primitive pairs); r = (ka*KB + kb)*NAB + ia*NB + jb,
+// kk = kc*KD + kd.
+template <int CX, int CY>
+__device__ __forceinline__ void eri_column(const BraStage& st, const double* __restrict__ rk, int nkp, int ic, int id,
+                                           const double* __restrict__ tab,
+                                           double (&v)[QClass<CX, CY>::NROW][QClass<CX, CY>::KCD]) {
+    using Q = QClass<CX, CY>;
+    using BE = BraE<Q::LA, Q::LB, 0>;
+    constexpr int LA = Q::LA, LB = Q::LB, LC = Q::LC, LD = Q::LD, LAB = Q::LAB, LCD = Q::LCD, L = Q::L;
+    // classes with L >= 6 keep their outer Hermite loops rolled (compile time)
+    constexpr int UH = L >= 6 ? 1 : 16;
+    const int cx = cart_x(LC, ic), cy = cart_y(LC, ic), cz = cart_z(LC, ic);
+    const int dx = cart_x(LD, id), dy = cart_y(LD, id), dz = cart_z(LD, id);
+    const double fcd = cart_norm(cx, cy, cz) * cart_norm(dx, dy, dz);
+#pragma unroll
+    for (int r = 0; r < Q::NROW; ++r)
+#pragma unroll
+        for (int k = 0; k < Q::KCD; ++k) v[r][k] = 0.0;
+    for (int ib = 0; ib < st.nbp; ++ib) {
+        const double* b = st.rec + (size_t)ib * PPW;
+        const double p = b[0] + b[1];
+        const double Px = b[3], Py = b[4], Pz = b[5];
+        double X[Q::NHB][Q::KCD];
+#pragma unroll
+        for (int h = 0; h < Q::NHB; ++h)
+#pragma unroll
+            for (int k = 0; k < Q::KCD; ++k) X[h][k] = 0.0;
+        for (int ik = 0; ik < nkp; ++ik) {
+            const double* k = rk + (size_t)ik * PPW;
+            const double q = __ldg(k) + __ldg(k + 1), oo2q = 0.5 / q;
+            // ket E coefficients of this column only (box t2 <= cx+dx, ...)
+            double ex[LCD + 1], ey[LCD + 1], ez[LCD + 1];
+            {
+                double e[LC + 1][LD + 1][LCD + 1];
+                hermite_e<LC, LD>(__ldg(k + 6), __ldg(k + 9), oo2q, __ldg(k + 2), e);
+#pragma unroll
+                for (int t = 0; t <= LCD; ++t) ex[t] = e[cx][dx][t];
+                hermite_e<LC, LD>(__ldg(k + 7), __ldg(k + 10), oo2q, 1.0, e);
+#pragma unroll
+                for (int t = 0; t <= LCD; ++t) ey[t] = e[cy][dy][t];
+                hermite_e<LC, LD>(__ldg(k + 8), __ldg(k + 11), oo2q, 1.0, e);
+#pragma unroll
+                for (int t = 0; t <= LCD; ++t) ez[t] = e[cz][dz][t];
+            }
+            const double alpha = p * q / (p + q);
+            const double pref = TWO_PI_2_5 / (p * q * sqrt(p + q)) * fcd;
+            double R[nherm(L)];
+            hermite_r<L>(alpha, Px - __ldg(k + 3), Py - __ldg(k + 4), Pz - __ldg(k + 5), tab, R);
+            double ck[Q::KCD];
+#pragma unroll
+            for (int i = 0; i < Q::KCD; ++i) ck[i] = __ldg(k + 12 + i) * pref;
+#pragma unroll UH
+            for (int t = 0; t <= LAB; ++t)
+#pragma unroll UH
+                for (int u = 0; u <= LAB - t; ++u)
+#pragma unroll
+                    for (int w = 0; w <= LAB - t - u; ++w) {
+                        double s = 0.0;
+#pragma unroll
+                        for (int t2 = 0; t2 <= LCD; ++t2) {
+                            if (t2 > cx + dx) continue;
+#pragma unroll
+                            for (int u2 = 0; u2 <= LCD; ++u2) {
+                                if (u2 > cy + dy) continue;
+                                const double exy = ((t2 + u2) & 1) ? -ex[t2] * ey[u2] : ex[t2] * ey[u2];
+#pragma unroll
+                                for (int v2 = 0; v2 <= LCD; ++v2) {
+                                    if (v2 > cz + dz) continue;
+                                    const double e = (v2 & 1) ? -exy * ez[v2] : exy * ez[v2];
+                                    s += e * R[hidx(t + t2, u + u2, w + v2)];
+                                }
+                            }
+                        }
+#pragma unroll
+                        for (int kk = 0; kk < Q::KCD; ++kk) X[hidx(t, u, w)][kk] += ck[kk] * s;
+                    }
+        }
+        // bra step: v[(ka,kb),ab][kk] += C_bp[ka,kb] f_ab sum_box E^{ab}_tuv X[tuv][kk]
+        const double* E = st.E + (size_t)ib * BE::SIZE;
+#pragma unroll UH
+        for (int ia = 0; ia < Q::NA; ++ia) {
+            const int ax = cart_x(LA, ia), ay = cart_y(LA, ia), az = cart_z(LA, ia);
+#pragma unroll
+            for (int jb = 0; jb < Q::NB; ++jb) {
+                const int bx = cart_x(LB, jb), by = cart_y(LB, jb), bz = cart_z(LB, jb);
+                const double fab = cart_norm(ax, ay, az) * cart_norm(bx, by, bz);
+                double s[Q::KCD];
+#pragma unroll
+                for (int kk = 0; kk < Q::KCD; ++kk) s[kk] = 0.0;
+#pragma unroll
+                for (int t = 0; t <= ax + bx; ++t)
+#pragma unroll
+                    for (int u = 0; u <= ay + by; ++u) {
+                        const double exy = E[BE::at(0, ax, bx, t)] * E[BE::at(1, ay, by, u)];
+#pragma unroll
+                        for (int w = 0; w <= az + bz; ++w) {
+                            const double e = exy * E[BE::at(2, az, bz, w)];
+#pragma unroll
+                            for (int kk = 0; kk < Q::KCD; ++kk) s[kk] += e * X[hidx(t, u, w)][kk];
+                        }
+                    }
+#pragma unroll
+                for (int kab = 0; kab < Q::KAB; ++kab) {
+                    const double c = b[12 + kab] * fab;
+#pragma unroll
+                    for (int kk = 0; kk < Q::KCD; ++kk) v[kab * Q::NAB + ia * Q::NB + jb][kk] += c * s[kk];
+                }
+            }
+        }
+    }
+}
+
+// Everything the quartet kernels share.
+struct QuartetArgs {
+    PairView pv;
+    BlockView bv;
+    const double* boys;
+    const int* sorted;          // [npair] pair index at sorted position
+    const double* sortedQ;      // [npair]
+    const int64_t* counts;      // [NCLS][npair + 1] kept ket prefix length per (ket class, bra position)
+    int npair;
+    int cls_start[NCLS + 1];    // sorted positions of each pair class
+    int nao;
+};
+
+__device__ __forceinline__ void load_stage(const QuartetArgs& a, int P1, BraStage& st, double* E) {
+    st.P1 = P1;
+    st.A = a.pv.pa_blk[P1];
+    st.B = a.pv.pb_blk[P1];
+    st.nbp = a.pv.npp[P1];
+    st.rec = a.pv.rec + a.pv.slot[P1] * PPW;
+    st.aA = a.bv.atom[st.A];
+    st.aB = a.bv.atom[st.B];
+    st.nA = a.bv.ncon[st.A];
+    st.nB = a.bv.ncon[st.B];
+    st.oA = a.bv.ao[st.A];
+    st.oB = a.bv.ao[st.B];
+    st.E = E;
+}
+
+struct JKArgs {
+    QuartetArgs q;
+    const double* D;    // [nset][nao][nao], symmetric
+    double* J;          // un-symmetrised accumulators, same shape
+    double* K;
+};
+
+// Digest one column (fixed ket component pair cd, all ket contractions kk)
+// of a quartet for NS densities. Each tensor element the block reaches is
+// visited n_gen = (A==B ? 2:1)(C==D ? 2:1)(P1==P2 ? 2:1) times under the 8
+// index maps, so each image carries g = 1/n_gen:
+//   J[m,n] += 2g v D[l,s],  J[l,s] += 2g v D[m,n]
+//   K[m,l] += g v D[n,s],   K[n,l] += g v D[m,s],  K[m,s] += g v D[n,l],  K[n,s] += g v D[m,l]
+// (m in A, n in B, l in C, s in D); the host forms J + J^T and K + K^T.
+// K rows m, n belong to the bra pair: Ksm[set][slot][col], slot < KA*NA for
+// A's functions, then B's.
+template <int CX, int CY, int NS>
+__device__ __forceinline__ void jk_digest_column(const JKArgs& a, const BraStage& st, int P2, int C, int Dd, int ic,
+                                                 int id, const double (&v)[QClass<CX, CY>::NROW][QClass<CX, CY>::KCD],
+                                                 double (&jab)[NS][QClass<CX, CY>::NROW], double* Ksm) {
+    using Q = QClass<CX, CY>;
+    const BlockView& bv = a.q.bv;
+    const int nC = bv.ncon[C], nD = bv.ncon[Dd], oC = bv.ao[C], oD = bv.ao[Dd];
+    const double g = 1.0 / ((st.A == st.B ? 2.0 : 1.0) * (C == Dd ? 2.0 : 1.0) * (st.P1 == P2 ? 2.0 : 1.0));
+    const int n = a.q.nao;
+    const size_t nn = (size_t)n * n;
+    constexpr int NFA = Q::KA * Q::NA;      // A slots, then B slots
+    constexpr int NF = NFA + Q::KB * Q::NB;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        const double* __restrict__ D = a.D + s * nn;
+        double* Ks = Ksm + (size_t)s * NF * n;
+#pragma unroll
+        for (int kc = 0; kc < Q::KC; ++kc)
+#pragma unroll
+            for (int kd = 0; kd < Q::KD; ++kd) {
+                if (kc >= nC || kd >= nD) continue;
+                const int kk = kc * Q::KD + kd;
+                const int l = oC + kc * Q::NC + ic, sg = oD + kd * Q::ND + id;
+                const double dls = __ldg(D + (size_t)l * n + sg);
+                double jcd = 0.0;
+#pragma unroll
+                for (int ka = 0; ka < Q::KA; ++ka)
+#pragma unroll
+                    for (int kb = 0; kb < Q::KB; ++kb) {
+                        if (ka >= st.nA || kb >= st.nB) continue;
+#pragma unroll
+                        for (int ia = 0; ia < Q::NA; ++ia)
+#pragma unroll
+                            for (int jb = 0; jb < Q::NB; ++jb) {
+                                const int r = (ka * Q::KB + kb) * Q::NAB + ia * Q::NB + jb;
+                                const int m = st.oA + ka * Q::NA + ia, nb_ = st.oB + kb * Q::NB + jb;
+                                jcd += v[r][kk] * __ldg(D + (size_t)m * n + nb_);
+                                jab[s][r] += 2.0 * g * v[r][kk] * dls;
+                            }
+                    }
+                atomicAdd(a.J + s * nn + (size_t)l * n + sg, 2.0 * g * jcd);
+                // K[m, l] and K[m, sg]: rows of A's functions
+#pragma unroll
+                for (int ka = 0; ka < Q::KA; ++ka)
+#pragma unroll
+                    for (int ia = 0; ia < Q::NA; ++ia) {
+                        if (ka >= st.nA) continue;
+                        double s1 = 0.0, s2 = 0.0;
+#pragma unroll
+                        for (int kb = 0; kb < Q::KB; ++kb)
+#pragma unroll
+                            for (int jb = 0; jb < Q::NB; ++jb) {
+                                if (kb >= st.nB) continue;
+                                const int r = (ka * Q::KB + kb) * Q::NAB + ia * Q::NB + jb;
+                                const size_t nb_ = st.oB + kb * Q::NB + jb;
+                                s1 += v[r][kk] * __ldg(D + nb_ * n + sg);
+                                s2 += v[r][kk] * __ldg(D + nb_ * n + l);
+                            }
+                        double* row = Ks + (size_t)(ka * Q::NA + ia) * n;
+                        atomicAdd(row + l, g * s1);
+                        atomicAdd(row + sg, g * s2);
+                    }
+                // K[n, l] and K[n, sg]: rows of B's functions
+#pragma unroll
+                for (int kb = 0; kb < Q::KB; ++kb)
+#pragma unroll
+                    for (int jb = 0; jb < Q::NB; ++jb) {
+                        if (kb >= st.nB) continue;
+                        double s1 = 0.0, s2 = 0.0;
+#pragma unroll
+                        for (int ka = 0; ka < Q::KA; ++ka)
+#pragma unroll
+                            for (int ia = 0; ia < Q::NA; ++ia) {
+                                if (ka >= st.nA) continue;
+                                const int r = (ka * Q::KB + kb) * Q::NAB + ia * Q::NB + jb;
+                                const size_t m = st.oA + ka * Q::NA + ia;
+                                s1 += v[r][kk] * __ldg(D + m * n + sg);
+                                s2 += v[r][kk] * __ldg(D + m * n + l);
+                            }
+                        double* row = Ks + (size_t)(NFA + kb * Q::NB + jb) * n;
+                        atomicAdd(row + l, g * s1);
+                        atomicAdd(row + sg, g * s2);
+                    }
+            }
+    }
+}
+
+// Items of ket class CY for the staged bra pair.
+template <int CX, int CY, int NS>
+__device__ __forceinline__ void jk_ket_class(const JKArgs& a, const BraStage& st, int spos,
+                                             double (&jab)[NS][QClass<CX, CY>::NROW], double* Ksm) {
+    using Q = QClass<CX, CY>;
+    const int64_t cnt = a.q.counts[(size_t)CY * (a.q.npair + 1) + spos];
+    const int j0 = a.q.cls_start[CY];
+    const int64_t items = cnt * Q::NCD;
+    for (int64_t it = threadIdx.x; it < items; it += blockDim.x) {
+        const int jj = static_cast<int>(it / Q::NCD), cd = static_cast<int>(it % Q::NCD);
+        const int P2 = a.q.sorted[j0 + jj];
+        const int C = a.q.pv.pa_blk[P2], Dd = a.q.pv.pb_blk[P2];
+        const int ic = cd / Q::ND, id = cd % Q::ND;
+        double v[Q::NROW][Q::KCD];
+        eri_column<CX, CY>(st, a.q.pv.rec + a.q.pv.slot[P2] * PPW, a.q.pv.npp[P2], ic, id, a.q.boys, v);
+        jk_digest_column<CX, CY, NS>(a, st, P2, C, Dd, ic, id, v, jab, Ksm);
+    }
+}
+
+template <int CX, int NS>
+struct JKKernel {
+    using Q0 = QClass<CX, 0>;
+    static constexpr int NROW = Q0::NROW;
+    static constexpr int NF = Q0::KA * Q0::NA + Q0::KB * Q0::NB;
+    static constexpr int ESIZE = BraE<Q0::LA, Q0::LB, 0>::SIZE;
+};
+
+// Dynamic shared memory: K rows [NS][NF][nao], J_ab [NS][NROW], bra E tables.
+template <int CX, int NS>
+__global__ void __launch_bounds__(128) jk_bra_kernel(JKArgs a) {
+    using KK = JKKernel<CX, NS>;
+    using Q0 = QClass<CX, 0>;
+    extern __shared__ double smem[];
+    const int n = a.q.nao;
+    double* Ksm = smem;
+    double* Jsm = Ksm + (size_t)NS * KK::NF * n;
+    double* Esm = Jsm + NS * KK::NROW;
+    const int spos = a.q.cls_start[CX] + blockIdx.x;
+    const int P1 = a.q.sorted[spos];
+    __shared__ BraStage st;
+    if (threadIdx.x == 0) load_stage(a.q, P1, st, Esm);
+    for (int i = threadIdx.x; i < NS * KK::NF * n + NS * KK::NROW; i += blockDim.x) smem[i] = 0.0;
+    __syncthreads();
+    stage_bra_e<Q0::LA, Q0::LB, 0>(st);
+    __syncthreads();
+    double jab[NS][KK::NROW];
+#pragma unroll
+    for (int s = 0; s < NS; ++s)
+#pragma unroll
+        for (int r = 0; r < KK::NROW; ++r) jab[s][r] = 0.0;
+    if (CX >= 0) jk_ket_class<CX, 0, NS>(a, st, spos, jab, Ksm);
+    if constexpr (CX >= 1) jk_ket_class<CX, 1, NS>(a, st, spos, jab, Ksm);
+    if constexpr (CX >= 2) jk_ket_class<CX, 2, NS>(a, st, spos, jab, Ksm);
+    if constexpr (CX >= 3) jk_ket_class<CX, 3, NS>(a, st, spos, jab, Ksm);
+    if constexpr (CX >= 4) jk_ket_class<CX, 4, NS>(a, st, spos, jab, Ksm);
+    if constexpr (CX >= 5) jk_ket_class<CX, 5, NS>(a, st, spos, jab, Ksm);
+#pragma unroll
+    for (int s = 0; s < NS; ++s)
+#pragma unroll
+        for (int r = 0; r < KK::NROW; ++r)
+            if (jab[s][r] != 0.0) atomicAdd(Jsm + s * KK::NROW + r, jab[s][r]);
+    __syncthreads();
+    const size_t nn = (size_t)n * n;
+    // flush J_ab
+    for (int i = threadIdx.x; i < NS * KK::NROW; i += blockDim.x) {
+        const double val = Jsm[i];
+        if (val == 0.0) continue;
+        const int s = i / KK::NROW, r = i % KK::NROW;
+        const int kab = r / Q0::NAB, ab = r % Q0::NAB;
+        const int ka = kab / Q0::KB, kb = kab % Q0::KB;
+        const int m = st.oA + ka * Q0::NA + ab / Q0::NB, nb_ = st.oB + kb * Q0::NB + ab % Q0::NB;
+        atomicAdd(a.J + s * nn + (size_t)m * n + nb_, val);
+    }
+    // flush K rows
+    constexpr int NFA = Q0::KA * Q0::NA;
+    for (int i = threadIdx.x; i < NS * KK::NF * n; i += blockDim.x) {
+        const double val = Ksm[i];
+        if (val == 0.0) continue;
+        const int col = i % n, f = (i / n) % KK::NF, s = i / (n * KK::NF);
+        const int row = f < NFA ? st.oA + (f / Q0::NA) * Q0::NA + f % Q0::NA
+                                : st.oB + ((f - NFA) / Q0::NB) * Q0::NB + (f - NFA) % Q0::NB;
+        atomicAdd(a.K + s * nn + (size_t)row * n + col, val);
+    }
+}
+
+template <int CX, int NS>
+size_t jk_smem_bytes(int nao, int max_bra_prims) {
+    using KK = JKKernel<CX, NS>;
+    return sizeof(double) * ((size_t)NS * KK::NF * nao + NS * KK::NROW + (size_t)max_bra_prims * KK::ESIZE);
+}
+
+// ---------------------------------------------------------- Schwarz
+
+// Q[P] = max_ab |(ab|ab)|^(1/2) (the reference's _schwarz_kernel,
+// aimd/qc/integrals.py:864-883): one CTA per pair, one thread per column.
+template <int CX>
+__global__ void __launch_bounds__(64) schwarz_kernel(QuartetArgs a, const int* pairs_of_class, double* Qout) {
+    using Q = QClass<CX, CX>;
+    extern __shared__ double smem[];
+    __shared__ BraStage st;
+    __shared__ unsigned long long qmax;
+    const int P = pairs_of_class[blockIdx.x];
+    if (threadIdx.x == 0) {
+        load_stage(a, P, st, smem);
+        qmax = 0ull;
+    }
+    __syncthreads();
+    stage_bra_e<Q::LA, Q::LB, 0>(st);
+    __syncthreads();
+    for (int cd = threadIdx.x; cd < Q::NCD; cd += blockDim.x) {
+        double v[Q::NROW][Q::KCD];
+        eri_column<CX, CX>(st, st.rec, st.nbp, cd / Q::ND, cd % Q::ND, a.boys, v);
+        double m = 0.0;
+#pragma unroll
+        for (int ka = 0; ka < Q::KA; ++ka)
+#pragma unroll
+            for (int kb = 0; kb < Q::KB; ++kb) {
+                if (ka >= st.nA || kb >= st.nB) continue;
+                const int kk = ka * Q::KB + kb;
+#pragma unroll
+                for (int r = 0; r < Q::NROW; ++r)
+                    if (r == kk * Q::NAB + cd) m = fmax(m, fabs(v[r][kk]));
+            }
+        atomicMax(&qmax, (unsigned long long)__double_as_longlong(m));   // m >= 0: bit order = value order
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) Qout[P] = sqrt(__longlong_as_double((long long)qmax));
+}
+
+}  // namespace hf

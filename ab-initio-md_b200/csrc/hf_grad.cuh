@@ -1,0 +1,318 @@
+// Integral-direct two-electron gradient 1/2 sum Gamma d(mn|ls)/dR.
+//
+// Same decomposition as the J/K build: one CTA per bra block pair, one
+// thread item per (ket pair, ket component pair cd). The quartet list is
+// enumerated at thr / Gamma_bound, so every quartet the exact test can keep
+// is visited; each item applies the reference's test Q1 Q2 max|Gamma| < thr
+// (aimd/qc/integrals.py:1329) to its column of Gamma.
+//
+//   Gamma_{mnls} = deg [Dc_mn Dc_ls - k/2 sum_x (Dx_ml Dx_ns + Dx_ms Dx_nl)],
+//   deg = 1/2 x (2 if A != B) x (2 if C != D) x (2 if P1 != P2)
+// (aimd/qc/integrals.py:1298-1328). Centres A and B: shifted bra Hermite
+// expansions d/dA_x -> 2a E^{i+1,j} - i E^{i-1,j} with R up to L + 1 (the
+// reference's _grad_pass, :1049-1244). Centre C: the same identity on the
+// ket expansion, contracted with the bra-transformed Gamma. Centre D:
+// translational invariance, -(A + B + C), per column.
+#pragma once
+#include "hf_eri.cuh"
+
+namespace hf {
+
+struct GradArgs {
+    QuartetArgs q;
+    const double* Dc;       // [nao][nao] symmetric
+    const double* Dx;       // [nx][nao][nao] symmetric
+    int nx;
+    double kfac;
+    double thr;             // exact screening threshold on Q1 Q2 max|Gamma|
+    double* grad;           // [natm][3]
+    int natm;
+};
+
+// Gradient contribution of one column; adds A, B parts to gab and C, D
+// parts to the shared accumulator gsh[natm][3].
+template <int CX, int CY>
+__device__ __forceinline__ void grad_column(const GradArgs& a, const BraStage& st, int P2, double QQ, int ic,
+                                            int id, double (&gab)[6], double* gsh) {
+    using Q = QClass<CX, CY>;
+    using BE = BraE<Q::LA, Q::LB, 1>;
+    constexpr int LA = Q::LA, LB = Q::LB, LC = Q::LC, LD = Q::LD, LAB = Q::LAB, LCD = Q::LCD, L = Q::L + 1;
+    constexpr int NH1 = nherm(LAB + 1);
+    constexpr int UH = L >= 5 ? 1 : 16;      // rolled outer Hermite loops for large classes
+    constexpr int UW = L >= 7 ? 1 : 16;      // and the inner one for the largest (compile time)
+    const BlockView& bv = a.q.bv;
+    const int C = a.q.pv.pa_blk[P2], Dd = a.q.pv.pb_blk[P2];
+    const int aC = bv.atom[C], aD = bv.atom[Dd];
+    if (st.aA == st.aB && st.aB == aC && aC == aD) return;          // one-centre: invariant
+    const int nC = bv.ncon[C], nD = bv.ncon[Dd], oC = bv.ao[C], oD = bv.ao[Dd];
+    const int n = a.q.nao;
+    const size_t nn = (size_t)n * n;
+    const double deg = 0.5 * (st.A != st.B ? 2.0 : 1.0) * (C != Dd ? 2.0 : 1.0) * (st.P1 != P2 ? 2.0 : 1.0);
+    // Gamma column
+    double G[Q::NROW][Q::KCD];
+    double gmax = 0.0;
+#pragma unroll
+    for (int kk = 0; kk < Q::KCD; ++kk) {
+        const int kc = kk / Q::KD, kd = kk % Q::KD;
+        const bool cv = kc < nC && kd < nD;
+        const size_t l = oC + kc * Q::NC + ic, sg = oD + kd * Q::ND + id;
+#pragma unroll
+        for (int r = 0; r < Q::NROW; ++r) {
+            const int kab = r / Q::NAB, ab = r % Q::NAB, ka = kab / Q::KB, kb = kab % Q::KB;
+            double val = 0.0;
+            if (cv && ka < st.nA && kb < st.nB) {
+                const size_t m = st.oA + ka * Q::NA + ab / Q::NB, nb_ = st.oB + kb * Q::NB + ab % Q::NB;
+                val = __ldg(a.Dc + m * n + nb_) * __ldg(a.Dc + l * n + sg);
+                for (int x = 0; x < a.nx; ++x) {
+                    const double* X = a.Dx + x * nn;
+                    val -= 0.5 * a.kfac * (__ldg(X + m * n + l) * __ldg(X + nb_ * n + sg) +
+                                           __ldg(X + m * n + sg) * __ldg(X + nb_ * n + l));
+                }
+                val *= deg;
+            }
+            G[r][kk] = val;
+            gmax = fmax(gmax, fabs(val));
+        }
+    }
+    if (QQ == 0.0 || QQ * gmax < a.thr) return;
+    double dA[3] = {0.0, 0.0, 0.0}, dB[3] = {0.0, 0.0, 0.0}, dC[3] = {0.0, 0.0, 0.0};
+    const int cx = cart_x(LC, ic), cy = cart_y(LC, ic), cz = cart_z(LC, ic);
+    const int dx = cart_x(LD, id), dy = cart_y(LD, id), dz = cart_z(LD, id);
+    const double fcd = cart_norm(cx, cy, cz) * cart_norm(dx, dy, dz);
+    const double* rk = a.q.pv.rec + a.q.pv.slot[P2] * PPW;
+    const int nkp = a.q.pv.npp[P2];
+    for (int ib = 0; ib < st.nbp; ++ib) {
+        const double* b = st.rec + (size_t)ib * PPW;
+        const double ea = b[0], eb = b[1], p = ea + eb;
+        const double* E = st.E + (size_t)ib * BE::SIZE;
+        // Gamma contracted with this bra primitive's coefficients (and f_ab),
+        // and its bra Hermite transform Y[h][kk] (for the C-centre pass)
+        double gb[Q::NAB][Q::KCD];
+        double Y[Q::NHB][Q::KCD];
+#pragma unroll
+        for (int h = 0; h < Q::NHB; ++h)
+#pragma unroll
+            for (int kk = 0; kk < Q::KCD; ++kk) Y[h][kk] = 0.0;
+#pragma unroll UH
+        for (int ia = 0; ia < Q::NA; ++ia) {
+            const int ax = cart_x(LA, ia), ay = cart_y(LA, ia), az = cart_z(LA, ia);
+#pragma unroll
+            for (int jb = 0; jb < Q::NB; ++jb) {
+                const int bx = cart_x(LB, jb), by = cart_y(LB, jb), bz = cart_z(LB, jb);
+                const double fab = cart_norm(ax, ay, az) * cart_norm(bx, by, bz);
+                const int ab = ia * Q::NB + jb;
+#pragma unroll
+                for (int kk = 0; kk < Q::KCD; ++kk) {
+                    double s = 0.0;
+#pragma unroll
+                    for (int kab = 0; kab < Q::KAB; ++kab) s += b[12 + kab] * G[kab * Q::NAB + ab][kk];
+                    gb[ab][kk] = s * fab;
+                }
+#pragma unroll
+                for (int t = 0; t <= ax + bx; ++t)
+#pragma unroll
+                    for (int u = 0; u <= ay + by; ++u)
+#pragma unroll
+                        for (int w = 0; w <= az + bz; ++w) {
+                            const double e = E[BE::at(0, ax, bx, t)] * E[BE::at(1, ay, by, u)] * E[BE::at(2, az, bz, w)];
+#pragma unroll
+                            for (int kk = 0; kk < Q::KCD; ++kk) Y[hidx(t, u, w)][kk] += e * gb[ab][kk];
+                        }
+            }
+        }
+        double Xb[NH1][Q::KCD];
+#pragma unroll
+        for (int h = 0; h < NH1; ++h)
+#pragma unroll
+            for (int kk = 0; kk < Q::KCD; ++kk) Xb[h][kk] = 0.0;
+        for (int ik = 0; ik < nkp; ++ik) {
+            const double* k = rk + (size_t)ik * PPW;
+            const double ec = __ldg(k), q = ec + __ldg(k + 1), oo2q = 0.5 / q;
+            // ket E for this column, and d/dC_d of it (one extra in direction d)
+            double ex[LCD + 2], ey[LCD + 2], ez[LCD + 2], gx[LCD + 2], gy[LCD + 2], gz[LCD + 2];
+            {
+                double e[LC + 2][LD + 1][LCD + 2];
+                hermite_e<LC + 1, LD>(__ldg(k + 6), __ldg(k + 9), oo2q, __ldg(k + 2), e);
+#pragma unroll
+                for (int t = 0; t <= LCD + 1; ++t) {
+                    ex[t] = t <= LCD ? e[cx][dx][t] : 0.0;
+                    gx[t] = 2.0 * ec * e[cx + 1][dx][t] - (cx > 0 ? cx * e[cx > 0 ? cx - 1 : 0][dx][t] : 0.0);
+                }
+                hermite_e<LC + 1, LD>(__ldg(k + 7), __ldg(k + 10), oo2q, 1.0, e);
+#pragma unroll
+                for (int t = 0; t <= LCD + 1; ++t) {
+                    ey[t] = t <= LCD ? e[cy][dy][t] : 0.0;
+                    gy[t] = 2.0 * ec * e[cy + 1][dy][t] - (cy > 0 ? cy * e[cy > 0 ? cy - 1 : 0][dy][t] : 0.0);
+                }
+                hermite_e<LC + 1, LD>(__ldg(k + 8), __ldg(k + 11), oo2q, 1.0, e);
+#pragma unroll
+                for (int t = 0; t <= LCD + 1; ++t) {
+                    ez[t] = t <= LCD ? e[cz][dz][t] : 0.0;
+                    gz[t] = 2.0 * ec * e[cz + 1][dz][t] - (cz > 0 ? cz * e[cz > 0 ? cz - 1 : 0][dz][t] : 0.0);
+                }
+            }
+            const double alpha = p * q / (p + q);
+            const double pref = TWO_PI_2_5 / (p * q * sqrt(p + q)) * fcd;
+            double R[nherm(L)];
+            hermite_r<L>(alpha, b[3] - __ldg(k + 3), b[4] - __ldg(k + 4), b[5] - __ldg(k + 5), a.q.boys, R);
+            double ck[Q::KCD];
+#pragma unroll
+            for (int i = 0; i < Q::KCD; ++i) ck[i] = __ldg(k + 12 + i) * pref;
+            // bra pass: Xb[h][kk] += sum_{k in box(cd)} (-1)^|k| E^{cd}_k R_{h+k} ck
+#pragma unroll UH
+            for (int t = 0; t <= LAB + 1; ++t)
+#pragma unroll UH
+                for (int u = 0; u <= LAB + 1 - t; ++u)
+#pragma unroll UW
+                    for (int w = 0; w <= LAB + 1 - t - u; ++w) {
+                        double s = 0.0;
+#pragma unroll
+                        for (int t2 = 0; t2 <= LCD; ++t2) {
+                            if (t2 > cx + dx) continue;
+#pragma unroll
+                            for (int u2 = 0; u2 <= LCD; ++u2) {
+                                if (u2 > cy + dy) continue;
+                                const double exy = ((t2 + u2) & 1) ? -ex[t2] * ey[u2] : ex[t2] * ey[u2];
+#pragma unroll
+                                for (int v2 = 0; v2 <= LCD; ++v2) {
+                                    if (v2 > cz + dz) continue;
+                                    s += ((v2 & 1) ? -exy * ez[v2] : exy * ez[v2]) * R[hidx(t + t2, u + u2, w + v2)];
+                                }
+                            }
+                        }
+#pragma unroll
+                        for (int kk = 0; kk < Q::KCD; ++kk) Xb[hidx(t, u, w)][kk] += ck[kk] * s;
+                    }
+            // C-centre pass: dC_d += sum_h sum_k (-1)^|k| dE^{cd}_{d,k} R_{h+k} (sum_kk Y[h][kk] ck[kk])
+#pragma unroll UH
+            for (int t = 0; t <= LAB; ++t)
+#pragma unroll UH
+                for (int u = 0; u <= LAB - t; ++u)
+#pragma unroll UW
+                    for (int w = 0; w <= LAB - t - u; ++w) {
+                        double yv = 0.0;
+#pragma unroll
+                        for (int kk = 0; kk < Q::KCD; ++kk) yv += Y[hidx(t, u, w)][kk] * ck[kk];
+                        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+#pragma unroll
+                        for (int t2 = 0; t2 <= LCD + 1; ++t2) {
+                            if (t2 > cx + dx + 1) continue;
+#pragma unroll
+                            for (int u2 = 0; u2 <= LCD + 1; ++u2) {
+                                if (u2 > cy + dy + 1) continue;
+#pragma unroll
+                                for (int v2 = 0; v2 <= LCD + 1; ++v2) {
+                                    if (v2 > cz + dz + 1) continue;
+                                    const int over = (t2 > cx + dx) + (u2 > cy + dy) + (v2 > cz + dz);
+                                    if (over > 1) continue;
+                                    const double r = ((t2 + u2 + v2) & 1) ? -R[hidx(t + t2, u + u2, w + v2)]
+                                                                          : R[hidx(t + t2, u + u2, w + v2)];
+                                    s0 += gx[t2] * ey[u2] * ez[v2] * r;
+                                    s1 += ex[t2] * gy[u2] * ez[v2] * r;
+                                    s2 += ex[t2] * ey[u2] * gz[v2] * r;
+                                }
+                            }
+                        }
+                        dC[0] += yv * s0;
+                        dC[1] += yv * s1;
+                        dC[2] += yv * s2;
+                    }
+        }
+        // bra pass, A and B: sum_ab sum_kk gb[ab][kk] sum_{h in dbox(ab)} dE_h Xb[h][kk]
+#pragma unroll UH
+        for (int ia = 0; ia < Q::NA; ++ia) {
+            const int ax = cart_x(LA, ia), ay = cart_y(LA, ia), az = cart_z(LA, ia);
+#pragma unroll
+            for (int jb = 0; jb < Q::NB; ++jb) {
+                const int bx = cart_x(LB, jb), by = cart_y(LB, jb), bz = cart_z(LB, jb);
+                const int ab = ia * Q::NB + jb;
+#pragma unroll
+                for (int t = 0; t <= ax + bx + 1; ++t)
+#pragma unroll
+                    for (int u = 0; u <= ay + by + 1; ++u)
+#pragma unroll
+                        for (int w = 0; w <= az + bz + 1; ++w) {
+                            const int over = (t > ax + bx) + (u > ay + by) + (w > az + bz);
+                            if (over > 1) continue;
+                            double yv = 0.0;
+#pragma unroll
+                            for (int kk = 0; kk < Q::KCD; ++kk) yv += gb[ab][kk] * Xb[hidx(t, u, w)][kk];
+                            const double e0 = E[BE::at(0, ax, bx, t)], e1 = E[BE::at(1, ay, by, u)],
+                                         e2 = E[BE::at(2, az, bz, w)];
+                            const double dax = 2.0 * ea * E[BE::at(0, ax + 1, bx, t)] - (ax > 0 ? ax * E[BE::at(0, ax > 0 ? ax - 1 : 0, bx, t)] : 0.0);
+                            const double day = 2.0 * ea * E[BE::at(1, ay + 1, by, u)] - (ay > 0 ? ay * E[BE::at(1, ay > 0 ? ay - 1 : 0, by, u)] : 0.0);
+                            const double daz = 2.0 * ea * E[BE::at(2, az + 1, bz, w)] - (az > 0 ? az * E[BE::at(2, az > 0 ? az - 1 : 0, bz, w)] : 0.0);
+                            const double dbx = 2.0 * eb * E[BE::at(0, ax, bx + 1, t)] - (bx > 0 ? bx * E[BE::at(0, ax, bx > 0 ? bx - 1 : 0, t)] : 0.0);
+                            const double dby = 2.0 * eb * E[BE::at(1, ay, by + 1, u)] - (by > 0 ? by * E[BE::at(1, ay, by > 0 ? by - 1 : 0, u)] : 0.0);
+                            const double dbz = 2.0 * eb * E[BE::at(2, az, bz + 1, w)] - (bz > 0 ? bz * E[BE::at(2, az, bz > 0 ? bz - 1 : 0, w)] : 0.0);
+                            dA[0] += yv * dax * e1 * e2;
+                            dA[1] += yv * e0 * day * e2;
+                            dA[2] += yv * e0 * e1 * daz;
+                            dB[0] += yv * dbx * e1 * e2;
+                            dB[1] += yv * e0 * dby * e2;
+                            dB[2] += yv * e0 * e1 * dbz;
+                        }
+            }
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        gab[d] += dA[d];
+        gab[3 + d] += dB[d];
+        atomicAdd(gsh + 3 * aC + d, dC[d]);
+        atomicAdd(gsh + 3 * aD + d, -(dA[d] + dB[d] + dC[d]));
+    }
+}
+
+template <int CX, int CY>
+__device__ __forceinline__ void grad_ket_class(const GradArgs& a, const BraStage& st, int spos, double (&gab)[6],
+                                               double* gsh) {
+    using Q = QClass<CX, CY>;
+    const int64_t cnt = a.q.counts[(size_t)CY * (a.q.npair + 1) + spos];
+    const int j0 = a.q.cls_start[CY];
+    const double q1 = a.q.sortedQ[spos];
+    for (int64_t it = threadIdx.x; it < cnt * Q::NCD; it += blockDim.x) {
+        const int jj = static_cast<int>(it / Q::NCD), cd = static_cast<int>(it % Q::NCD);
+        const int P2 = a.q.sorted[j0 + jj];
+        grad_column<CX, CY>(a, st, P2, q1 * a.q.sortedQ[j0 + jj], cd / Q::ND, cd % Q::ND, gab, gsh);
+    }
+}
+
+// Dynamic shared memory: gradient accumulator [natm][3], bra E tables (+1).
+template <int CX>
+__global__ void __launch_bounds__(128) grad2e_bra_kernel(GradArgs a) {
+    using Q0 = QClass<CX, 0>;
+    extern __shared__ double smem[];
+    double* gsh = smem;
+    double* Esm = smem + 3 * a.natm;
+    __shared__ BraStage st;
+    const int spos = a.q.cls_start[CX] + blockIdx.x;
+    if (threadIdx.x == 0) load_stage(a.q, a.q.sorted[spos], st, Esm);
+    for (int i = threadIdx.x; i < 3 * a.natm; i += blockDim.x) gsh[i] = 0.0;
+    __syncthreads();
+    stage_bra_e<Q0::LA, Q0::LB, 1>(st);
+    __syncthreads();
+    double gab[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    grad_ket_class<CX, 0>(a, st, spos, gab, gsh);
+    if constexpr (CX >= 1) grad_ket_class<CX, 1>(a, st, spos, gab, gsh);
+    if constexpr (CX >= 2) grad_ket_class<CX, 2>(a, st, spos, gab, gsh);
+    if constexpr (CX >= 3) grad_ket_class<CX, 3>(a, st, spos, gab, gsh);
+    if constexpr (CX >= 4) grad_ket_class<CX, 4>(a, st, spos, gab, gsh);
+    if constexpr (CX >= 5) grad_ket_class<CX, 5>(a, st, spos, gab, gsh);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        if (gab[d] != 0.0) atomicAdd(gsh + 3 * st.aA + d, gab[d]);
+        if (gab[3 + d] != 0.0) atomicAdd(gsh + 3 * st.aB + d, gab[3 + d]);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 3 * a.natm; i += blockDim.x)
+        if (gsh[i] != 0.0) atomicAdd(a.grad + i, gsh[i]);
+}
+
+template <int CX>
+size_t grad_smem_bytes(int natm, int max_bra_prims) {
+    using Q0 = QClass<CX, 0>;
+    return sizeof(double) * (3 * (size_t)natm + (size_t)max_bra_prims * BraE<Q0::LA, Q0::LB, 1>::SIZE);
+}
+
+}  // namespace hf

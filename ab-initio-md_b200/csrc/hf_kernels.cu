@@ -1,0 +1,608 @@
+// B200 (sm_100a) Hartree-Fock integral engine: C-ABI entry points.
+//
+// A context owns the device copy of one basis (contraction blocks for the
+// two-electron kernels, segmented shells for the one-electron kernels) and
+// every geometry-dependent buffer (primitive-pair records, Schwarz bounds,
+// the class-sorted pair order and the quartet prefix scans). All device
+// memory is allocated in aimd_create; the per-step calls allocate nothing
+// and run on the caller's stream.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "../../include/aimd_b200.h"
+#include "hf_launch.h"
+
+using namespace hf;
+
+namespace {
+
+#define CK(call)                                                     \
+    do {                                                             \
+        cudaError_t e_ = (call);                                     \
+        if (e_ != cudaSuccess) {                                     \
+            snprintf(g_err, sizeof g_err, "%s: %s", #call, cudaGetErrorString(e_)); \
+            return AIMD_ERR_CUDA;                                    \
+        }                                                            \
+    } while (0)
+
+thread_local char g_err[512] = "";
+
+// Boys table F_n(0.1 k), n < BOYS_COLS: the positive series for a high order
+// (all terms positive, no cancellation), then downward recursion.
+std::vector<double> boys_table() {
+    const int top = 32;
+    std::vector<double> t(BOYS_NGRID * BOYS_COLS);
+    std::vector<double> col(top + 1);
+    for (int k = 0; k < BOYS_NGRID; ++k) {
+        const double x = 0.1 * k;
+        double term = 1.0 / (2 * top + 1), total = term;
+        for (int j = 1; j < 400; ++j) {
+            term = term * (2.0 * x) / (2 * top + 2 * j + 1);
+            total += term;
+        }
+        const double ex = std::exp(-x);
+        col[top] = ex * total;
+        for (int n = top - 1; n >= 0; --n) col[n] = (2.0 * x * col[n + 1] + ex) / (2 * n + 1);
+        for (int n = 0; n < BOYS_COLS; ++n) t[k * BOYS_COLS + n] = col[n];
+    }
+    return t;
+}
+
+template <typename T>
+cudaError_t dalloc(T** p, size_t n) { return cudaMalloc(reinterpret_cast<void**>(p), std::max<size_t>(n, 1) * sizeof(T)); }
+
+}  // namespace
+
+struct aimd_ctx {
+    int natm, nao, nblock, nshell, npair, nspair;
+    int nsm;
+    // blocks
+    int *blk_atom, *blk_l, *blk_ncon, *blk_ao, *blk_p0, *blk_np;
+    double *blk_exp, *blk_coef;
+    // shells (one-electron)
+    int *sh_atom, *sh_l, *sh_ao, *sh_p0, *sh_np, *sp_i, *sp_j;
+    double *sh_exp, *sh_coef, *charges;
+    int sp_cls_start[7];
+    // pairs
+    int *pa, *pb, *npp;
+    int64_t* slot;
+    double* rec;
+    int64_t nrec;
+    double* Q;
+    int cls_start[NCLS + 1];
+    int* by_class;          // pair indices grouped by class (static)
+    int* seg_begin;         // cub segment offsets
+    double* keys_in;
+    double* sortedQ;
+    int* sorted;
+    int64_t* counts_jk;     // [NCLS][npair + 1] kept ket prefix per (ket class, bra position)
+    int64_t* counts_g;
+    int maxbp[NCLS];        // largest primitive-pair count of a block pair, per class
+    double thr_jk = -1.0, thr_g = -1.0;
+    void* cub_tmp;
+    size_t cub_bytes;
+    double* boys;
+    double* pos;            // [natm][3] device copy of the current geometry
+    bool have_geometry = false;
+    uint64_t launches = 0;
+};
+
+extern "C" const char* aimd_last_error(void) { return g_err; }
+
+extern "C" int aimd_create(aimd_ctx** out, int natm, int nao, int nblock, const int* blk_atom, const int* blk_l,
+                           const int* blk_ncon, const int* blk_ao, const int* blk_p0, const int* blk_np, int nbprim,
+                           const double* blk_exp, const double* blk_coef, int nshell, const int* sh_atom,
+                           const int* sh_l, const int* sh_ao, const int* sh_p0, const int* sh_np, int nsprim,
+                           const double* sh_exp, const double* sh_coef, const double* charges) {
+    if (!out || natm <= 0 || nao <= 0 || nblock <= 0 || nshell <= 0) {
+        snprintf(g_err, sizeof g_err, "aimd_create: empty basis");
+        return AIMD_ERR_ARG;
+    }
+    for (int b = 0; b < nblock; ++b)
+        if (blk_l[b] < 0 || blk_l[b] > LMAX || blk_ncon[b] < 1 || blk_ncon[b] > ncon_cap(blk_l[b])) {
+            snprintf(g_err, sizeof g_err, "aimd_create: block %d has l=%d ncon=%d (supported l<=%d, ncon<=cap)", b,
+                     blk_l[b], blk_ncon[b], LMAX);
+            return AIMD_ERR_UNSUPPORTED;
+        }
+    for (int s = 0; s < nshell; ++s)
+        if (sh_l[s] < 0 || sh_l[s] > LMAX) {
+            snprintf(g_err, sizeof g_err, "aimd_create: shell %d has l=%d > %d", s, sh_l[s], LMAX);
+            return AIMD_ERR_UNSUPPORTED;
+        }
+    auto* c = new aimd_ctx();
+    c->natm = natm;
+    c->nao = nao;
+    c->nblock = nblock;
+    c->nshell = nshell;
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, dev));
+    auto up_i = [&](int** d, const int* h, size_t n) -> cudaError_t {
+        cudaError_t e = dalloc(d, n);
+        if (e != cudaSuccess) return e;
+        return cudaMemcpy(*d, h, n * sizeof(int), cudaMemcpyHostToDevice);
+    };
+    auto up_d = [&](double** d, const double* h, size_t n) -> cudaError_t {
+        cudaError_t e = dalloc(d, n);
+        if (e != cudaSuccess) return e;
+        return cudaMemcpy(*d, h, n * sizeof(double), cudaMemcpyHostToDevice);
+    };
+    CK(up_i(&c->blk_atom, blk_atom, nblock));
+    CK(up_i(&c->blk_l, blk_l, nblock));
+    CK(up_i(&c->blk_ncon, blk_ncon, nblock));
+    CK(up_i(&c->blk_ao, blk_ao, nblock));
+    CK(up_i(&c->blk_p0, blk_p0, nblock));
+    CK(up_i(&c->blk_np, blk_np, nblock));
+    CK(up_d(&c->blk_exp, blk_exp, nbprim));
+    CK(up_d(&c->blk_coef, blk_coef, 2 * (size_t)nbprim));
+    CK(up_i(&c->sh_atom, sh_atom, nshell));
+    CK(up_i(&c->sh_l, sh_l, nshell));
+    CK(up_i(&c->sh_ao, sh_ao, nshell));
+    CK(up_i(&c->sh_p0, sh_p0, nshell));
+    CK(up_i(&c->sh_np, sh_np, nshell));
+    CK(up_d(&c->sh_exp, sh_exp, nsprim));
+    CK(up_d(&c->sh_coef, sh_coef, nsprim));
+    CK(up_d(&c->charges, charges, natm));
+    {   // Boys table
+        std::vector<double> t = boys_table();
+        CK(up_d(&c->boys, t.data(), t.size()));
+    }
+    CK(dalloc(&c->pos, 3 * (size_t)natm));
+    // shell pairs (si >= sj) grouped by class (l_i >= l_j after orientation)
+    {
+        std::vector<int> pi, pj;
+        int k = 0;
+        for (int cl = 0; cl < NCLS; ++cl) {
+            c->sp_cls_start[cl] = k;
+            for (int i = 0; i < nshell; ++i)
+                for (int j = 0; j <= i; ++j) {
+                    int a = i, b = j;
+                    if (sh_l[a] < sh_l[b]) std::swap(a, b);
+                    if (pcls(sh_l[a], sh_l[b]) != cl) continue;
+                    pi.push_back(a);
+                    pj.push_back(b);
+                    ++k;
+                }
+        }
+        c->sp_cls_start[NCLS] = k;
+        c->nspair = k;
+        CK(up_i(&c->sp_i, pi.data(), pi.size()));
+        CK(up_i(&c->sp_j, pj.data(), pj.size()));
+    }
+    // block pairs: orientation, class, record slots
+    {
+        const int np = nblock * (nblock + 1) / 2;
+        c->npair = np;
+        std::vector<int> pa(np), pb(np), cls(np);
+        std::vector<int64_t> slot(np);
+        int64_t nrec = 0;
+        int ip = 0;
+        for (int i = 0; i < nblock; ++i)
+            for (int j = 0; j <= i; ++j, ++ip) {
+                int a = i, b = j;
+                if (blk_l[a] < blk_l[b]) std::swap(a, b);
+                pa[ip] = a;
+                pb[ip] = b;
+                cls[ip] = pcls(blk_l[a], blk_l[b]);
+                slot[ip] = nrec;
+                nrec += (int64_t)blk_np[a] * blk_np[b];
+            }
+        c->nrec = nrec;
+        std::vector<int> by;
+        by.reserve(np);
+        for (int cl = 0; cl < NCLS; ++cl) {
+            c->cls_start[cl] = (int)by.size();
+            for (int p = 0; p < np; ++p)
+                if (cls[p] == cl) by.push_back(p);
+        }
+        c->cls_start[NCLS] = np;
+        std::vector<int> seg(c->cls_start, c->cls_start + NCLS + 1);
+        CK(up_i(&c->pa, pa.data(), np));
+        CK(up_i(&c->pb, pb.data(), np));
+        CK(up_i(&c->by_class, by.data(), np));
+        CK(up_i(&c->seg_begin, seg.data(), NCLS + 1));
+        CK(dalloc(&c->slot, np));
+        CK(cudaMemcpy(c->slot, slot.data(), np * sizeof(int64_t), cudaMemcpyHostToDevice));
+        CK(dalloc(&c->npp, np));
+        CK(dalloc(&c->rec, (size_t)nrec * PPW));
+        CK(dalloc(&c->Q, np));
+        CK(dalloc(&c->keys_in, np));
+        CK(dalloc(&c->sortedQ, np));
+        CK(dalloc(&c->sorted, np));
+        CK(dalloc(&c->counts_jk, (size_t)NCLS * (np + 1)));
+        CK(dalloc(&c->counts_g, (size_t)NCLS * (np + 1)));
+        for (int cl = 0; cl < NCLS; ++cl) c->maxbp[cl] = 1;
+        for (int p = 0; p < np; ++p)
+            c->maxbp[cls[p]] = std::max(c->maxbp[cls[p]], blk_np[pa[p]] * blk_np[pb[p]]);
+        size_t b1 = 0;
+        CK(cub::DeviceSegmentedRadixSort::SortPairsDescending(nullptr, b1, c->keys_in, c->sortedQ, c->by_class,
+                                                               c->sorted, np, NCLS, c->seg_begin, c->seg_begin + 1));
+        c->cub_bytes = b1;
+        CK(cudaMalloc(&c->cub_tmp, c->cub_bytes));
+    }
+    *out = c;
+    return AIMD_OK;
+}
+
+extern "C" int aimd_destroy(aimd_ctx* c) {
+    if (!c) return AIMD_OK;
+    void* ptrs[] = {c->blk_atom, c->blk_l, c->blk_ncon, c->blk_ao, c->blk_p0, c->blk_np, c->blk_exp, c->blk_coef,
+                    c->sh_atom, c->sh_l, c->sh_ao, c->sh_p0, c->sh_np, c->sp_i, c->sp_j, c->sh_exp, c->sh_coef,
+                    c->charges, c->pa, c->pb, c->npp, c->slot, c->rec, c->Q, c->by_class, c->seg_begin,
+                    c->keys_in, c->sortedQ, c->sorted, c->counts_jk, c->counts_g, c->cub_tmp, c->boys, c->pos};
+    for (void* p : ptrs) cudaFree(p);
+    delete c;
+    return AIMD_OK;
+}
+
+// ------------------------------------------------------------ geometry
+
+namespace {
+
+// Primitive pairs of each block pair with mu |A-B|^2 <= 50 (the reference's
+// PRIM_CUTOFF, aimd/qc/integrals.py:506-510), compacted into the pair's slot.
+__global__ void pair_prep_kernel(int npair, const int* pa, const int* pb, const int64_t* slot, const int* blk_atom,
+                                 const int* blk_l, const int* blk_p0, const int* blk_np, const double* exps,
+                                 const double* coefs, const double* pos, int* npp, double* rec) {
+    const int ip = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ip >= npair) return;
+    const int A = pa[ip], B = pb[ip];
+    const int iA = blk_atom[A], iB = blk_atom[B];
+    const double ABx = pos[3 * iA] - pos[3 * iB], ABy = pos[3 * iA + 1] - pos[3 * iB + 1],
+                 ABz = pos[3 * iA + 2] - pos[3 * iB + 2];
+    const double r2 = ABx * ABx + ABy * ABy + ABz * ABz;
+    const int kB = ncon_cap(blk_l[B]);
+    double* out = rec + slot[ip] * PPW;
+    int n = 0;
+    for (int ka = blk_p0[A]; ka < blk_p0[A] + blk_np[A]; ++ka) {
+        const double a = exps[ka];
+        for (int kb = blk_p0[B]; kb < blk_p0[B] + blk_np[B]; ++kb) {
+            const double b = exps[kb], p = a + b, mu = a * b / p;
+            if (!(mu * r2 <= 50.0)) continue;
+            double* r = out + (size_t)n * PPW;
+            const double bp = b / p, ap = a / p;
+            r[0] = a;
+            r[1] = b;
+            r[2] = exp(-mu * r2);
+            r[3] = pos[3 * iA] - bp * ABx;
+            r[4] = pos[3 * iA + 1] - bp * ABy;
+            r[5] = pos[3 * iA + 2] - bp * ABz;
+            r[6] = -bp * ABx;
+            r[7] = -bp * ABy;
+            r[8] = -bp * ABz;
+            r[9] = ap * ABx;
+            r[10] = ap * ABy;
+            r[11] = ap * ABz;
+            for (int i = 0; i < 4; ++i) r[12 + i] = 0.0;
+            for (int ca = 0; ca < ncon_cap(blk_l[A]); ++ca)
+                for (int cb = 0; cb < kB; ++cb) r[12 + ca * kB + cb] = coefs[2 * ka + ca] * coefs[2 * kb + cb];
+            ++n;
+        }
+    }
+    npp[ip] = n;
+}
+
+__global__ void gather_keys_kernel(int n, const int* by_class, const double* Q, double* keys) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) keys[i] = Q[by_class[i]];
+}
+
+struct ClsStart { int v[NCLS + 1]; };
+
+// counts[Y][s] = number of ket pairs of class Y (sorted prefix) kept with the
+// bra at sorted position s (class X >= Y), Q_s Q_j >= thr; cut at s for Y == X.
+__global__ void quartet_count_kernel(int npair, ClsStart cs, const double* sortedQ, double thr, int64_t* counts) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s > npair) return;
+    if (s == npair) {
+        for (int y = 0; y < NCLS; ++y) counts[(size_t)y * (npair + 1) + npair] = 0;
+        return;
+    }
+    int X = 0;
+    while (s >= cs.v[X + 1]) ++X;
+    const double qs = sortedQ[s];
+    for (int y = 0; y < NCLS; ++y) {
+        int64_t cnt = 0;
+        if (y <= X) {
+            int lo = cs.v[y], hi = cs.v[y + 1];       // first j with qs*Q_j < thr
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (qs * sortedQ[mid] >= thr) lo = mid + 1; else hi = mid;
+            }
+            cnt = lo - cs.v[y];
+            if (y == X && cnt > s - cs.v[X] + 1) cnt = s - cs.v[X] + 1;
+        }
+        counts[(size_t)y * (npair + 1) + s] = cnt;
+    }
+}
+
+PairView pair_view(aimd_ctx* c) { return PairView{c->pa, c->pb, c->slot, c->npp, c->rec}; }
+BlockView block_view(aimd_ctx* c) { return BlockView{c->blk_atom, c->blk_l, c->blk_ncon, c->blk_ao}; }
+
+QuartetArgs quartet_args(aimd_ctx* c, const int64_t* counts) {
+    QuartetArgs q;
+    q.pv = pair_view(c);
+    q.bv = block_view(c);
+    q.boys = c->boys;
+    q.sorted = c->sorted;
+    q.sortedQ = c->sortedQ;
+    q.counts = counts;
+    q.npair = c->npair;
+    for (int i = 0; i <= NCLS; ++i) q.cls_start[i] = c->cls_start[i];
+    q.nao = c->nao;
+    return q;
+}
+
+int build_counts(aimd_ctx* c, double thr, int64_t* counts, cudaStream_t st) {
+    ClsStart cs;
+    for (int i = 0; i <= NCLS; ++i) cs.v[i] = c->cls_start[i];
+    const int n = c->npair + 1;
+    quartet_count_kernel<<<(n + 127) / 128, 128, 0, st>>>(c->npair, cs, c->sortedQ, thr, counts);
+    ++c->launches;
+    CK(cudaGetLastError());
+    return AIMD_OK;
+}
+
+int ncls_pairs(aimd_ctx* c, int cl) { return c->cls_start[cl + 1] - c->cls_start[cl]; }
+
+LaunchEnv launch_env(aimd_ctx* c) {
+    LaunchEnv e;
+    for (int cl = 0; cl < NCLS; ++cl) {
+        e.cls_count[cl] = ncls_pairs(c, cl);
+        e.maxbp[cl] = c->maxbp[cl];
+    }
+    for (int cl = 0; cl <= NCLS; ++cl) e.cls_start[cl] = c->cls_start[cl];
+    e.nao = c->nao;
+    e.natm = c->natm;
+    e.by_class = c->by_class;
+    e.Q = c->Q;
+    return e;
+}
+
+int class_status(aimd_ctx* c, cudaError_t r, const char* what, int cl) {
+    if (r == cudaSuccess) {
+        if (c->cls_start[cl + 1] > c->cls_start[cl]) ++c->launches;
+        return AIMD_OK;
+    }
+    if (r == cudaErrorInvalidConfiguration) {
+        snprintf(g_err, sizeof g_err, "%s (pair class %d): shared memory beyond the 227 KB per-CTA limit "
+                 "(too many AOs for the K-row accumulator)", what, cl);
+        return AIMD_ERR_UNSUPPORTED;
+    }
+    snprintf(g_err, sizeof g_err, "%s (pair class %d): %s", what, cl, cudaGetErrorString(r));
+    return AIMD_ERR_CUDA;
+}
+
+#define AIMD_EACH_CLASS(CALL, WHAT)                                         \
+    do {                                                                    \
+        int r_;                                                             \
+        if ((r_ = class_status(c, CALL(0), WHAT, 0))) return r_;            \
+        if ((r_ = class_status(c, CALL(1), WHAT, 1))) return r_;            \
+        if ((r_ = class_status(c, CALL(2), WHAT, 2))) return r_;            \
+        if ((r_ = class_status(c, CALL(3), WHAT, 3))) return r_;            \
+        if ((r_ = class_status(c, CALL(4), WHAT, 4))) return r_;            \
+        if ((r_ = class_status(c, CALL(5), WHAT, 5))) return r_;            \
+    } while (0)
+
+}  // namespace
+
+extern "C" int aimd_set_geometry(aimd_ctx* c, const double* pos, void* stream) {
+    if (!c || !pos) return AIMD_ERR_ARG;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    CK(cudaMemcpyAsync(c->pos, pos, 3 * sizeof(double) * c->natm, cudaMemcpyDefault, st));
+    const int np = c->npair;
+    pair_prep_kernel<<<(np + 127) / 128, 128, 0, st>>>(np, c->pa, c->pb, c->slot, c->blk_atom, c->blk_l, c->blk_p0,
+                                                        c->blk_np, c->blk_exp, c->blk_coef, c->pos, c->npp, c->rec);
+    ++c->launches;
+    CK(cudaGetLastError());
+    {
+        const LaunchEnv e = launch_env(c);
+        const QuartetArgs q = quartet_args(c, c->counts_jk);
+#define AIMD_SCHWARZ(X) launch_schwarz_c##X(e, q, st)
+        AIMD_EACH_CLASS(AIMD_SCHWARZ, "aimd_set_geometry/schwarz");
+#undef AIMD_SCHWARZ
+    }
+    gather_keys_kernel<<<(np + 127) / 128, 128, 0, st>>>(np, c->by_class, c->Q, c->keys_in);
+    ++c->launches;
+    size_t bytes = c->cub_bytes;
+    CK(cub::DeviceSegmentedRadixSort::SortPairsDescending(c->cub_tmp, bytes, c->keys_in, c->sortedQ, c->by_class,
+                                                           c->sorted, np, NCLS, c->seg_begin, c->seg_begin + 1, 0,
+                                                           sizeof(double) * 8, st));
+    ++c->launches;
+    c->thr_jk = c->thr_g = -1.0;
+    c->have_geometry = true;
+    return AIMD_OK;
+}
+
+extern "C" int aimd_schwarz(aimd_ctx* c, double* Q, void* stream) {
+    if (!c || !Q || !c->have_geometry) return AIMD_ERR_ARG;
+    CK(cudaMemcpyAsync(Q, c->Q, sizeof(double) * c->npair, cudaMemcpyDefault, static_cast<cudaStream_t>(stream)));
+    return AIMD_OK;
+}
+
+extern "C" int aimd_pair_count(aimd_ctx* c) { return c ? c->npair : 0; }
+
+extern "C" int aimd_jk(aimd_ctx* c, int nset, const double* D, double* J, double* K, double thr, void* stream) {
+    if (!c || !D || !J || !K || nset < 1 || !c->have_geometry) return AIMD_ERR_ARG;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (thr != c->thr_jk) {
+        if (int r = build_counts(c, thr, c->counts_jk, st)) return r;
+        c->thr_jk = thr;
+    }
+    const size_t nn = (size_t)c->nao * c->nao;
+    CK(cudaMemsetAsync(J, 0, sizeof(double) * nset * nn, st));
+    CK(cudaMemsetAsync(K, 0, sizeof(double) * nset * nn, st));
+    // one pass per density (UHF: alpha and beta)
+    const LaunchEnv e = launch_env(c);
+    for (int s0 = 0; s0 < nset; ++s0) {
+        JKArgs a;
+        a.q = quartet_args(c, c->counts_jk);
+        a.D = D + s0 * nn;
+        a.J = J + s0 * nn;
+        a.K = K + s0 * nn;
+#define AIMD_JK(X) launch_jk_c##X(e, a, st)
+        AIMD_EACH_CLASS(AIMD_JK, "aimd_jk");
+#undef AIMD_JK
+    }
+    return AIMD_OK;
+}
+
+namespace {
+// unit symmetric density D_ls = D_sl = 1/2 (l != s), D_ll = 1
+__global__ void unit_density_kernel(int n, int l, int s, double* D) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * n) return;
+    const int r = i / n, c = i % n;
+    D[i] = ((r == l && c == s) || (r == s && c == l)) ? (l == s ? 1.0 : 0.5) : 0.0;
+}
+// eri[m][n][l][s] = eri[m][n][s][l] = J[m][n] + J[n][m]
+__global__ void scatter_slice_kernel(int n, int l, int s, const double* J, double* eri) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * n) return;
+    const size_t m = i / n, nn_ = i % n, N = n;
+    const double v = J[m * N + nn_] + J[nn_ * N + m];
+    eri[((m * N + nn_) * N + l) * N + s] = v;
+    eri[((m * N + nn_) * N + s) * N + l] = v;
+}
+}  // namespace
+
+// Test and debug sizes only: the tensor is probed column by column through
+// the integral-direct Coulomb build (J[D] with D the symmetric unit matrix
+// of (l, s) gives (mn|ls)); scratch for D/J/K is allocated here.
+extern "C" int aimd_eri_tensor(aimd_ctx* c, double* eri, double thr, void* stream) {
+    if (!c || !eri || !c->have_geometry) return AIMD_ERR_ARG;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int n = c->nao;
+    const size_t nn = (size_t)n * n;
+    double* scratch = nullptr;
+    CK(cudaMalloc(&scratch, 3 * nn * sizeof(double)));
+    double *D = scratch, *J = scratch + nn, *K = scratch + 2 * nn;
+    int status = AIMD_OK;
+    const int blocks = (int)((nn + 255) / 256);
+    for (int l = 0; l < n && status == AIMD_OK; ++l)
+        for (int s = 0; s <= l && status == AIMD_OK; ++s) {
+            unit_density_kernel<<<blocks, 256, 0, st>>>(n, l, s, D);
+            ++c->launches;
+            status = aimd_jk(c, 1, D, J, K, thr, stream);
+            if (status == AIMD_OK) {
+                scatter_slice_kernel<<<blocks, 256, 0, st>>>(n, l, s, J, eri);
+                ++c->launches;
+            }
+        }
+    cudaError_t e1 = cudaStreamSynchronize(st);
+    cudaFree(scratch);
+    if (status != AIMD_OK) return status;
+    CK(e1);
+    return AIMD_OK;
+}
+
+extern "C" int aimd_grad2e(aimd_ctx* c, const double* Dc, int nx, const double* Dx, double kfac, double thr,
+                           double gamma_bound, double* grad, void* stream) {
+    if (!c || !Dc || (nx > 0 && !Dx) || !grad || !c->have_geometry || !(gamma_bound > 0.0)) return AIMD_ERR_ARG;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // enumerate every quartet that can pass Q1 Q2 max|Gamma| >= thr
+    const double thr_enum = thr / gamma_bound;
+    if (thr_enum != c->thr_g) {
+        if (int r = build_counts(c, thr_enum, c->counts_g, st)) return r;
+        c->thr_g = thr_enum;
+    }
+    CK(cudaMemsetAsync(grad, 0, sizeof(double) * 3 * c->natm, st));
+    GradArgs a;
+    a.q = quartet_args(c, c->counts_g);
+    a.Dc = Dc;
+    a.Dx = Dx;
+    a.nx = nx;
+    a.kfac = kfac;
+    a.thr = thr;
+    a.grad = grad;
+    a.natm = c->natm;
+    const LaunchEnv e = launch_env(c);
+#define AIMD_GRAD(X) launch_grad_c##X(e, a, st)
+    AIMD_EACH_CLASS(AIMD_GRAD, "aimd_grad2e");
+#undef AIMD_GRAD
+    return AIMD_OK;
+}
+
+namespace {
+ShellView shell_view(aimd_ctx* c) {
+    ShellView s;
+    s.nshell = c->nshell;
+    s.natm = c->natm;
+    s.nao = c->nao;
+    s.atom = c->sh_atom;
+    s.l = c->sh_l;
+    s.ao = c->sh_ao;
+    s.p0 = c->sh_p0;
+    s.np = c->sh_np;
+    s.exps = c->sh_exp;
+    s.coefs = c->sh_coef;
+    s.pos = c->pos;
+    s.charges = c->charges;
+    s.pair_i = c->sp_i;
+    s.pair_j = c->sp_j;
+    return s;
+}
+}  // namespace
+
+extern "C" int aimd_onee(aimd_ctx* c, const double* origin, double* S, double* T, double* M, double* V,
+                         void* stream) {
+    if (!c || !S || !T || !M || !V || !c->have_geometry) return AIMD_ERR_ARG;
+    int n = 0;
+    cudaError_t r = launch_onee(launch_env(c), shell_view(c), c->sp_cls_start, origin, c->boys, S, T, M, V,
+                                static_cast<cudaStream_t>(stream), &n);
+    c->launches += n;
+    CK(r);
+    return AIMD_OK;
+}
+
+extern "C" int aimd_onee_grad(aimd_ctx* c, const double* W, const double* D, double* grad, void* stream) {
+    if (!c || !W || !D || !grad || !c->have_geometry) return AIMD_ERR_ARG;
+    int n = 0;
+    cudaError_t r = launch_onee_grad(launch_env(c), shell_view(c), c->sp_cls_start, c->boys, W, D, grad,
+                                     static_cast<cudaStream_t>(stream), &n);
+    c->launches += n;
+    if (r == cudaErrorInvalidConfiguration) {
+        snprintf(g_err, sizeof g_err, "aimd_onee_grad: too many atoms for the shared accumulator");
+        return AIMD_ERR_UNSUPPORTED;
+    }
+    CK(r);
+    return AIMD_OK;
+}
+
+extern "C" int aimd_quartet_counts(aimd_ctx* c, int which, int64_t* out_host) {
+    // kept quartets per class pair (bra class X, ket class Y <= X), 6 x 6
+    // row-major, for the J/K list (which = 0) or the gradient list (which = 1)
+    if (!c || !out_host || !c->have_geometry) return AIMD_ERR_ARG;
+    const int64_t* counts = which ? c->counts_g : c->counts_jk;
+    const int n = c->npair + 1;
+    std::vector<int64_t> h((size_t)NCLS * n);
+    CK(cudaMemcpy(h.data(), counts, sizeof(int64_t) * h.size(), cudaMemcpyDeviceToHost));
+    for (int x = 0; x < NCLS; ++x)
+        for (int y = 0; y < NCLS; ++y) {
+            int64_t t = 0;
+            if (y <= x)
+                for (int s = c->cls_start[x]; s < c->cls_start[x + 1]; ++s) t += h[(size_t)y * n + s];
+            out_host[x * NCLS + y] = t;
+        }
+    return AIMD_OK;
+}
+
+extern "C" int aimd_pair_data(aimd_ctx* c, int* npp_host, int* cls_host, int* sorted_host) {
+    // per pair: surviving primitive pairs; per sorted position: class and pair index
+    if (!c || !c->have_geometry) return AIMD_ERR_ARG;
+    if (npp_host) CK(cudaMemcpy(npp_host, c->npp, sizeof(int) * c->npair, cudaMemcpyDeviceToHost));
+    if (sorted_host) CK(cudaMemcpy(sorted_host, c->sorted, sizeof(int) * c->npair, cudaMemcpyDeviceToHost));
+    if (cls_host)
+        for (int cl = 0; cl < NCLS; ++cl)
+            for (int s = c->cls_start[cl]; s < c->cls_start[cl + 1]; ++s) cls_host[s] = cl;
+    return AIMD_OK;
+}
+
+extern "C" uint64_t aimd_launch_count(aimd_ctx* c) { return c ? c->launches : 0; }
+
+extern "C" int aimd_version(void) { return AIMD_ABI_VERSION; }

@@ -1,0 +1,46 @@
+// Host-side launchers of the class-templated kernels. Each bra pair class
+// lives in its own translation units (hf_class_jk.cu and hf_class_grad.cu
+// compiled with -DAIMD_CLASS=0..5) so that they compile in parallel.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "hf_grad.cuh"
+#include "hf_onee.cuh"
+
+namespace hf {
+
+struct LaunchEnv {
+    int cls_count[NCLS];     // block pairs per class
+    int cls_start[NCLS + 1]; // start of each class in the class-grouped order
+    int maxbp[NCLS];         // largest primitive-pair count of a block pair, per class
+    int nao, natm;
+    const int* by_class;     // pair indices grouped by class
+    double* Q;
+};
+
+// Status: cudaSuccess, a CUDA error, or cudaErrorInvalidConfiguration when
+// the shared-memory request exceeds the per-CTA limit.
+#define AIMD_DECLARE_CLASS(X)                                                                          \
+    cudaError_t launch_schwarz_c##X(const LaunchEnv& e, const QuartetArgs& q, cudaStream_t st);         \
+    cudaError_t launch_jk_c##X(const LaunchEnv& e, const JKArgs& a, cudaStream_t st);                    \
+    cudaError_t launch_grad_c##X(const LaunchEnv& e, const GradArgs& a, cudaStream_t st);
+AIMD_DECLARE_CLASS(0)
+AIMD_DECLARE_CLASS(1)
+AIMD_DECLARE_CLASS(2)
+AIMD_DECLARE_CLASS(3)
+AIMD_DECLARE_CLASS(4)
+AIMD_DECLARE_CLASS(5)
+#undef AIMD_DECLARE_CLASS
+
+cudaError_t launch_onee(const LaunchEnv& e, const ShellView& sv, const int* sp_cls_start, const double* origin,
+                        const double* boys, double* S, double* T, double* M, double* V, cudaStream_t st, int* nlaunch);
+cudaError_t launch_onee_grad(const LaunchEnv& e, const ShellView& sv, const int* sp_cls_start, const double* boys,
+                             const double* W, const double* D, double* grad, cudaStream_t st, int* nlaunch);
+
+inline cudaError_t set_smem_limit(const void* kernel, size_t bytes) {
+    if (bytes > 227 * 1024) return cudaErrorInvalidConfiguration;
+    if (bytes > 48 * 1024) return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    return cudaSuccess;
+}
+
+}  // namespace hf

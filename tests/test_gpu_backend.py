@@ -1,0 +1,119 @@
+"""
+The ForceBackend boundary on the GPU: the density-guess protocol, shape
+checks and error behaviour of the reference's hf backend
+(tests/test_hf_backend.py of the reference), analytic vs finite-difference
+gradients, and short NVE / XL-BOMD runs.
+"""
+
+import numpy as np
+import pytest
+
+from aimd_b200 import geometry as G
+
+pytestmark = pytest.mark.gpu
+
+
+def _backend(sym, basis, **kw):
+    from aimd_b200.backend import HFGPUBackend
+    return HFGPUBackend(sym, basis=basis, **kw)
+
+
+def test_h2_sto3g_literature_energy():
+    be = _backend(["H", "H"], "sto-3g")
+    r = be.compute(np.array([[0.0, 0.0, 0.0], [1.4, 0.0, 0.0]]))
+    assert r.energy == pytest.approx(-1.1167, abs=1e-4)
+    assert r.converged and r.density.shape == (2, 2)
+
+
+def test_density_guess_protocol():
+    sym, pos = G.water()
+    be = _backend(sym, "6-31g*")
+    r0 = be.compute(pos)
+    assert r0.info["guess"] == "init"
+    r1 = be.compute(pos + 0.01)
+    assert r1.info["guess"] == "previous"
+    be.set_density_guess(r0.density)
+    r2 = be.compute(pos)
+    assert r2.info["guess"] == "external"
+    r3 = be.compute(pos)
+    assert r3.info["guess"] == "previous"          # external guess used for one call only
+    assert abs(r2.energy - r0.energy) < 1e-9
+    with pytest.raises(ValueError):
+        be.set_density_guess(np.zeros((3, 3)))
+    with pytest.raises(ValueError):
+        be.set_density_guess(np.full(be.density_shape, np.nan))
+    with pytest.raises(ValueError):
+        be.compute(pos[:2])
+
+
+def test_unconverged_is_flagged_not_raised():
+    sym, pos = G.water()
+    be = _backend(sym, "6-31g*", max_cycles=2)
+    r = be.compute(pos)
+    assert not r.converged
+    assert r.info["warnings"]
+
+
+def test_uhf_methyl_radical(golden):
+    g = golden("ch3_uhf_631gs")
+    be = _backend([str(s) for s in g["symbols"]], "6-31g*", multiplicity=2)
+    r = be.compute(g["positions"])
+    assert r.density.shape == (2, 21, 21)
+    assert abs(r.energy - float(g["energy"])) < 1e-9
+    np.testing.assert_allclose(r.gradient, g["gradient"], atol=1e-7)
+    assert r.info["s2"] == pytest.approx(float(g["s2"]), abs=1e-8)
+
+
+def test_methanol_gradient_vs_central_differences():
+    sym, pos = G.methanol()
+    be = _backend(sym, "6-31g**", conv_tol=1e-12, conv_tol_grad=1e-9)
+    g = be.compute(pos).gradient
+    rng = np.random.default_rng(7)
+    h = 1e-4
+    for a in rng.choice(len(sym), size=3, replace=False):
+        for k in range(3):
+            xp, xm = pos.copy(), pos.copy()
+            xp[a, k] += h
+            xm[a, k] -= h
+            fd = (be.compute(xp).energy - be.compute(xm).energy) / (2 * h)
+            assert abs(fd - g[a, k]) < 1e-6, (a, k, fd, g[a, k])
+
+
+def test_translational_and_rotational_invariance():
+    from aimd_b200.gradients import invariance_residuals
+    sym, pos = G.methanol()
+    g = _backend(sym, "6-31g**", conv_tol_grad=1e-9).compute(pos).gradient
+    f, t = invariance_residuals(pos, g)
+    assert np.abs(f).max() < 1e-10
+    assert np.abs(t).max() < 1e-8
+
+
+def test_nve_and_xlbomd_short_runs():
+    from aimd_b200 import md as MD
+    sym, pos = G.water()
+    v = MD.maxwell_boltzmann(sym, 300.0, seed=1)
+    run = MD.XLBOMDRun(_backend(sym, "6-31g*"), sym, pos, v, 0.5, xl=False)
+    e0 = run.conserved_energy()
+    for _ in range(20):
+        run.step()
+    assert abs(run.conserved_energy() - e0) < 5e-5
+    run = MD.XLBOMDRun(_backend(sym, "6-31g*"), sym, pos, v, 0.5, k=5, xl=True)
+    e0 = run.conserved_energy()
+    for _ in range(20):
+        r = run.step()
+        assert r.info["guess"] == "external"
+    assert abs(run.conserved_energy() - e0) < 5e-5
+
+
+def test_device_md_matches_backend_md():
+    from aimd_b200 import md as MD
+    from aimd_b200.scf import SCFOptions, SCFSolver
+    sym, pos = G.water()
+    v = MD.maxwell_boltzmann(sym, 300.0, seed=3)
+    host = MD.XLBOMDRun(_backend(sym, "6-31g*"), sym, pos, v, 0.5, k=5, xl=True)
+    dev = MD.DeviceXLBOMD(SCFSolver(sym, "6-31g*", options=SCFOptions(warn_unconverged=False)), sym, pos, v, 0.5, k=5)
+    for _ in range(5):
+        host.step()
+        dev.step()
+    np.testing.assert_allclose(dev.x, host.x, atol=1e-8)
+    assert abs(dev.state.energy - host.result.energy) < 1e-8
