@@ -125,7 +125,7 @@ class Engine:
             x = positions.detach().to(self.device, torch.float64).reshape(self.natm, 3)
             key = x.cpu().numpy().tobytes()
         else:
-            arr = np.ascontiguousarray(np.asarray(positions, dtype=float).reshape(self.natm, 3))
+            arr = np.array(positions, dtype=float).reshape(self.natm, 3)
             key = arr.tobytes()
             x = torch.from_numpy(arr).to(self.device)
         if key == self._pos_key:
