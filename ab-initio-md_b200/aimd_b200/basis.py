@@ -157,6 +157,9 @@ class BasisSet:
                 rng[a] = (idx[0], idx[-1] + 1)
         self.atom_ao = _frozen(rng)
         self._group_blocks()
+        # state shared by every geometry of this basis (with_positions copies
+        # the reference): the device engine lives here
+        self._shared: dict = {}
         self._set_positions(positions)
 
     # ------------------------------------------------------------------ blocks

@@ -2,8 +2,8 @@
 Build the native library ``_native/libaimd_b200.so`` for sm_100a.
 
 The class-templated kernels are split into one translation unit per bra pair
-class (csrc/hf_class_jk.cu and hf_class_grad.cu, each compiled with
--DAIMD_CLASS=0..5) plus the
+class (csrc/hf_class_jk.cu, -DAIMD_CLASS=0..5) and per (bra, ket) class pair
+for the gradient (csrc/hf_class_grad.cu, -DAIMD_CLASS=X -DAIMD_KET=Y) plus the
 one-electron unit and the C-ABI unit, compiled in parallel and linked with
 the static CUDA runtime. Objects are rebuilt only when a source is newer.
 
@@ -32,10 +32,12 @@ FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std
 
 
 def _units() -> list[tuple[str, str, list[str]]]:
-    units = []
-    for kind in ("jk", "grad"):
-        units += [(os.path.join(CSRC, f"hf_class_{kind}.cu"), os.path.join(OBJ_DIR, f"hf_class_{kind}_{x}.o"),
-                   [f"-DAIMD_CLASS={x}"]) for x in range(6)]
+    units = [(os.path.join(CSRC, "hf_class_jk.cu"), os.path.join(OBJ_DIR, f"hf_class_jk_{x}.o"),
+              [f"-DAIMD_CLASS={x}"]) for x in range(6)]
+    units += [(os.path.join(CSRC, "hf_class_grad.cu"), os.path.join(OBJ_DIR, f"hf_class_grad_{x}_{y}.o"),
+               [f"-DAIMD_CLASS={x}", f"-DAIMD_KET={y}"]) for x in range(6) for y in range(x + 1)]
+    # slowest units first so the parallel build finishes sooner
+    units.sort(key=lambda u: -sum(int(f.split("=")[1]) for f in u[2]))
     units.append((os.path.join(CSRC, "hf_onee.cu"), os.path.join(OBJ_DIR, "hf_onee.o"), []))
     units.append((os.path.join(CSRC, "hf_kernels.cu"), os.path.join(OBJ_DIR, "hf_kernels.o"), []))
     return units

@@ -210,9 +210,9 @@ class Engine:
 
 def engine_for(basis: BasisSet) -> Engine:
     """The engine shared by every geometry of this basis (BasisSet.with_positions copies it)."""
-    eng = basis.__dict__.get("_engine")
+    eng = basis._shared.get("engine")
     if eng is None:
         eng = Engine(basis)
-        basis.__dict__["_engine"] = eng
+        basis._shared["engine"] = eng
     eng.set_geometry(basis.positions)
     return eng

@@ -15,7 +15,7 @@ using Q0 = QClass<CX, 0>;
 cudaError_t AIMD_CAT(launch_schwarz_c, AIMD_CLASS)(const LaunchEnv& e, const QuartetArgs& q, cudaStream_t st) {
     const int cnt = e.cls_count[CX];
     if (cnt == 0) return cudaSuccess;
-    const size_t smem = sizeof(double) * (size_t)e.maxbp[CX] * BraE<Q0::LA, Q0::LB, 0>::SIZE;
+    const size_t smem = sizeof(double) * (size_t)e.maxbp[CX] * (BraE<Q0::LA, Q0::LB, 0>::SIZE + SBW);
     cudaError_t r = set_smem_limit((const void*)schwarz_kernel<CX>, smem);
     if (r != cudaSuccess) return r;
     schwarz_kernel<CX><<<cnt, 64, smem, st>>>(q, e.by_class + e.cls_start[CX], e.Q);

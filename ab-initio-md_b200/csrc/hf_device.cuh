@@ -1,9 +1,8 @@
 // Device building blocks of the McMurchie-Davidson integrals (sm_100a).
 //
-// Boys function F_n(x): grid table (step 0.1) + Taylor series about the
-// nearest grid point for x < 40, asymptotic F_0 and upward recursion above
-// (Helgaker, Jorgensen & Olsen 2000, sec. 9.8.2; the reference's
-// aimd/qc/boys.py:88-114). Hermite expansion coefficients E^{ij}_t by the
+// Boys function F_n(x): positive power series (small x) or erf + upward
+// recursion (x >= n + 1.5), without tables (Helgaker, Jorgensen & Olsen
+// 2000, sec. 9.8; the reference tabulates, aimd/qc/boys.py:88-114). Hermite expansion coefficients E^{ij}_t by the
 // Obara-Saika-type recursion of McMurchie & Davidson (aimd/qc/hermite.py:110),
 // Hermite Coulomb integrals R_tuv by the level recursion, evaluated in place
 // (aimd/qc/hermite.py:145).
@@ -17,8 +16,6 @@
 namespace hf {
 
 constexpr int LMAX = 2;            // s, p, d: every built-in basis set
-constexpr int BOYS_COLS = 20;      // F_0..F_19 tabulated: orders up to 10 + 9 Taylor terms
-constexpr int BOYS_NGRID = 402;    // x_k = 0.1 k, k < 402
 constexpr int PPW = 16;            // doubles per primitive-pair record
 constexpr double PI = 3.14159265358979323846;
 constexpr double TWO_PI_2_5 = 34.98683665524972;   // 2 pi^(5/2)
@@ -54,6 +51,16 @@ __host__ __device__ constexpr int pcls(int la, int lb) { return la * (la + 1) / 
 __host__ __device__ constexpr int cls_la(int c) { return c == 0 ? 0 : (c < 3 ? 1 : 2); }
 __host__ __device__ constexpr int cls_lb(int c) { return c - pcls(cls_la(c), 0); }
 constexpr int NCLS = 6;
+// Sub-classes: within an angular class, pairs are grouped by their number of
+// surviving primitive pairs (buckets 1, 2-3, 4-7, 8-15, 16-31, 32+) and by
+// their contraction-combination count (1, 2, 4), so that the lanes of a warp
+// walk loops of similar length. Segment id = class * NSUB + sub.
+constexpr int NPPB = 6, NCONB = 3, NSUB = NPPB * NCONB, NSEG = NCLS * NSUB;
+__host__ __device__ inline int npp_bucket(int npp) {
+    int b = 0;
+    while (b < NPPB - 1 && npp >= (2 << b)) ++b;
+    return b;
+}
 
 // Normalisation of Cartesian component (lx, ly, lz) relative to x^l:
 // sqrt((2l-1)!! / ((2lx-1)!! (2ly-1)!! (2lz-1)!!)).
@@ -64,22 +71,39 @@ __host__ __device__ inline double cart_norm(int lx, int ly, int lz) {
 
 // ---------------------------------------------------------------- Boys
 
-// F_n(x) for one order n <= 10.
-__device__ __forceinline__ double boys_top(int n, double x, const double* __restrict__ tab) {
-    if (x < 40.0) {
-        const int k = static_cast<int>(x * 10.0 + 0.5);
-        const double dx = k * 0.1 - x;
-        const double* row = tab + k * BOYS_COLS + n;
-        // Horner form of sum_m F_{n+m}(x_k) dx^m / m!, m < 10
-        double acc = __ldg(row + 9);
+// Coefficient a_k of the positive series F_N(x) = e^{-x} sum_k a_k (2x)^k,
+// a_k = 1 / ((2N+1)(2N+3)...(2N+2k+1)).
+__host__ __device__ constexpr double boys_series_coef(int N, int k) {
+    double a = 1.0;
+    for (int j = 0; j <= k; ++j) a /= (2 * N + 2 * j + 1);
+    return a;
+}
+
+// F_N(x) without tables (no memory traffic in the integral loops):
+//   x <  N + 1.5: the positive series above in Horner form, 22 + 2N terms
+//                 (relative truncation < 1e-15 on the whole interval);
+//   x >= N + 1.5: F_0 = sqrt(pi/x) erf(sqrt(x)) / 2 and the upward recursion
+//                 F_{m+1} = ((2m+1) F_m - e^{-x}) / (2x), stable there
+//                 (measured relative error < 1.5e-15 for N <= 10).
+// Both are standard evaluations of F_N (Helgaker, Jorgensen & Olsen 2000,
+// sec. 9.8); the reference tabulates instead (aimd/qc/boys.py:88-114).
+// ex = e^{-x} is passed in by the caller, which needs it anyway.
+template <int N>
+__device__ __forceinline__ double boys_top(double x, double ex) {
+    if (x < N + 1.5) {
+        constexpr int NT = 22 + 2 * N;
+        const double y = 2.0 * x;
+        double s = boys_series_coef(N, NT - 1);
 #pragma unroll
-        for (int m = 8; m >= 0; --m) acc = __ldg(row + m) + acc * dx * (1.0 / (m + 1));
-        return acc;
+        for (int k = NT - 2; k >= 0; --k) s = fma(s, y, boys_series_coef(N, k));
+        return ex * s;
     }
-    double f = 0.5 * sqrt(PI / x);
-    if (n > 0) {
-        const double ex = exp(-x), inv2x = 0.5 / x;
-        for (int m = 0; m < n; ++m) f = ((2 * m + 1) * f - ex) * inv2x;
+    const double sx = sqrt(x);
+    double f = 0.88622692545275801365 * erf(sx) / sx;      // sqrt(pi)/2 erf(sqrt x)/sqrt x
+    if (N > 0) {
+        const double inv2x = 0.5 / x;
+#pragma unroll
+        for (int m = 0; m < N; ++m) f = ((2 * m + 1) * f - ex) * inv2x;
     }
     return f;
 }
@@ -88,11 +112,10 @@ __device__ __forceinline__ double boys_top(int n, double x, const double* __rest
 // overwriting the previous one in decreasing Hermite index (entries h only
 // read lower indices of the level above). R[0] of level n is (-2a)^n F_n.
 template <int L>
-__device__ __forceinline__ void hermite_r(double alpha, double X, double Y, double Z,
-                                          const double* __restrict__ tab, double (&R)[nherm(L)]) {
+__device__ __forceinline__ void hermite_r(double alpha, double X, double Y, double Z, double (&R)[nherm(L)]) {
     const double T = alpha * (X * X + Y * Y + Z * Z);
-    double f = boys_top(L, T, tab);
-    const double ex = (L > 0) ? exp(-T) : 0.0;
+    const double ex = exp(-T);
+    double f = boys_top<L>(T, ex);
     const double m2a = -2.0 * alpha;
     double pw[L + 1];
     pw[0] = 1.0;

@@ -30,6 +30,10 @@ struct QClass {
     static constexpr int KA = ncon_cap(LA), KB = ncon_cap(LB), KC = ncon_cap(LC), KD = ncon_cap(LD);
     static constexpr int KAB = KA * KB, KCD = KC * KD;
     static constexpr int NROW = KAB * NAB;
+    // ket contraction combinations per thread item: all of them unless the
+    // per-thread accumulator v[NROW][KG] would exceed 48 doubles
+    static constexpr int KG = NROW * KCD <= 48 ? KCD : ((KCD % 2 == 0 && NROW * 2 <= 48) ? 2 : 1);
+    static constexpr int NKG = KCD / KG;
     static constexpr int NHB = nherm(LAB);
 };
 
@@ -42,14 +46,16 @@ struct BraE {
 };
 
 // Shared-memory stage of one bra pair.
+constexpr int SBW = 12;     // per bra primitive: p, 1/p, Px, Py, Pz, a, b, -, c0..c3
 struct BraStage {
     int P1, A, B, nbp, aA, aB;
     int nA, nB, oA, oB;
     const double* rec;      // bra primitive records (global)
     double* E;              // [nbp][BraE::SIZE] (shared)
+    double* SB;             // [nbp][SBW] (shared)
 };
 
-// Fill stage->E for all bra primitives (block-cooperative).
+// Fill the shared stage (E tables and scalars) for all bra primitives.
 template <int LA, int LB, int G>
 __device__ __forceinline__ void stage_bra_e(const BraStage& st) {
     using BE = BraE<LA, LB, G>;
@@ -67,15 +73,65 @@ __device__ __forceinline__ void stage_bra_e(const BraStage& st) {
 #pragma unroll
                 for (int t = 0; t < LA + LB + 1 + 2 * G; ++t) out[BE::at(d, i, j, t)] = e[i][j][t];
     }
+    for (int ib = threadIdx.x; ib < st.nbp; ib += blockDim.x) {
+        const double* b = st.rec + (size_t)ib * PPW;
+        double* o = st.SB + (size_t)ib * SBW;
+        const double p = b[0] + b[1];
+        o[0] = p;
+        o[1] = 1.0 / p;
+        o[2] = b[3];
+        o[3] = b[4];
+        o[4] = b[5];
+        o[5] = b[0];
+        o[6] = b[1];
+        o[7] = 0.0;
+        o[8] = b[12];
+        o[9] = b[13];
+        o[10] = b[14];
+        o[11] = b[15];
+    }
 }
 
-// v[r][kk] = (row r | cd, contraction kk) of the quartet (bra stage, ket pair
-// records rk with nkp primitive pairs); r = (ka*KB + kb)*NAB + ia*NB + jb,
-// kk = kc*KD + kd.
+// One primitive-pair record of a ket pair (16 doubles, 128-byte aligned),
+// loaded with 16-byte vector loads.
+struct KetRec {
+    double a, b, K, Qx, Qy, Qz, QAx, QAy, QAz, QBx, QBy, QBz, c[4];
+};
+__device__ __forceinline__ KetRec load_ket(const double* __restrict__ rec) {
+    const double2* r2 = reinterpret_cast<const double2*>(rec);
+    KetRec k;
+    double2 v = __ldg(r2 + 0); k.a = v.x; k.b = v.y;
+    v = __ldg(r2 + 1); k.K = v.x; k.Qx = v.y;
+    v = __ldg(r2 + 2); k.Qy = v.x; k.Qz = v.y;
+    v = __ldg(r2 + 3); k.QAx = v.x; k.QAy = v.y;
+    v = __ldg(r2 + 4); k.QAz = v.x; k.QBx = v.y;
+    v = __ldg(r2 + 5); k.QBy = v.x; k.QBz = v.y;
+    v = __ldg(r2 + 6); k.c[0] = v.x; k.c[1] = v.y;
+    v = __ldg(r2 + 7); k.c[2] = v.x; k.c[3] = v.y;
+    return k;
+}
+
+// out[t] = e[i][j][t] for runtime (i, j), by predicated copies (no local memory).
+template <int IM, int JM, int T>
+__device__ __forceinline__ void select_row(const double (&e)[IM + 1][JM + 1][T + 1], int i, int j, double (&out)[T + 1]) {
+#pragma unroll
+    for (int t = 0; t <= T; ++t) out[t] = 0.0;
+#pragma unroll
+    for (int ii = 0; ii <= IM; ++ii)
+#pragma unroll
+        for (int jj = 0; jj <= JM; ++jj)
+            if (ii == i && jj == j)
+#pragma unroll
+                for (int t = 0; t <= T; ++t) out[t] = e[ii][jj][t];
+}
+
+// v[r][kk] = (row r | cd, contraction kk) of the quartet (staged bra pair,
+// ket pair records rk with nkp primitive pairs); r = (ka*KB + kb)*NAB +
+// ia*NB + jb, kk = kc*KD + kd. Ket primitives outermost (each record is read
+// once), bra primitives inner (shared-memory broadcast).
 template <int CX, int CY>
 __device__ __forceinline__ void eri_column(const BraStage& st, const double* __restrict__ rk, int nkp, int ic, int id,
-                                           const double* __restrict__ tab,
-                                           double (&v)[QClass<CX, CY>::NROW][QClass<CX, CY>::KCD]) {
+                                           int kg, double (&v)[QClass<CX, CY>::NROW][QClass<CX, CY>::KG]) {
     using Q = QClass<CX, CY>;
     using BE = BraE<Q::LA, Q::LB, 0>;
     constexpr int LA = Q::LA, LB = Q::LB, LC = Q::LC, LD = Q::LD, LAB = Q::LAB, LCD = Q::LCD, L = Q::L;
@@ -87,40 +143,39 @@ __device__ __forceinline__ void eri_column(const BraStage& st, const double* __r
 #pragma unroll
     for (int r = 0; r < Q::NROW; ++r)
 #pragma unroll
-        for (int k = 0; k < Q::KCD; ++k) v[r][k] = 0.0;
-    for (int ib = 0; ib < st.nbp; ++ib) {
-        const double* b = st.rec + (size_t)ib * PPW;
-        const double p = b[0] + b[1];
-        const double Px = b[3], Py = b[4], Pz = b[5];
-        double X[Q::NHB][Q::KCD];
+        for (int k = 0; k < Q::KG; ++k) v[r][k] = 0.0;
+    for (int ik = 0; ik < nkp; ++ik) {
+        const KetRec k = load_ket(rk + (size_t)ik * PPW);
+        const double q = k.a + k.b, oo2q = 0.5 / q, iq = 2.0 * oo2q;
+        // ket E coefficients of this column only (box t2 <= cx+dx, ...)
+        double ex[LCD + 1], ey[LCD + 1], ez[LCD + 1];
+        {
+            double e[LC + 1][LD + 1][LCD + 1];
+            hermite_e<LC, LD>(k.QAx, k.QBx, oo2q, k.K, e);
+            select_row<LC, LD, LCD>(e, cx, dx, ex);
+            hermite_e<LC, LD>(k.QAy, k.QBy, oo2q, 1.0, e);
+            select_row<LC, LD, LCD>(e, cy, dy, ey);
+            hermite_e<LC, LD>(k.QAz, k.QBz, oo2q, 1.0, e);
+            select_row<LC, LD, LCD>(e, cz, dz, ez);
+        }
+        double ck[Q::KG];
 #pragma unroll
-        for (int h = 0; h < Q::NHB; ++h)
+        for (int i = 0; i < Q::KG; ++i) {
+            double c = k.c[0];
 #pragma unroll
-            for (int k = 0; k < Q::KCD; ++k) X[h][k] = 0.0;
-        for (int ik = 0; ik < nkp; ++ik) {
-            const double* k = rk + (size_t)ik * PPW;
-            const double q = __ldg(k) + __ldg(k + 1), oo2q = 0.5 / q;
-            // ket E coefficients of this column only (box t2 <= cx+dx, ...)
-            double ex[LCD + 1], ey[LCD + 1], ez[LCD + 1];
-            {
-                double e[LC + 1][LD + 1][LCD + 1];
-                hermite_e<LC, LD>(__ldg(k + 6), __ldg(k + 9), oo2q, __ldg(k + 2), e);
-#pragma unroll
-                for (int t = 0; t <= LCD; ++t) ex[t] = e[cx][dx][t];
-                hermite_e<LC, LD>(__ldg(k + 7), __ldg(k + 10), oo2q, 1.0, e);
-#pragma unroll
-                for (int t = 0; t <= LCD; ++t) ey[t] = e[cy][dy][t];
-                hermite_e<LC, LD>(__ldg(k + 8), __ldg(k + 11), oo2q, 1.0, e);
-#pragma unroll
-                for (int t = 0; t <= LCD; ++t) ez[t] = e[cz][dz][t];
-            }
-            const double alpha = p * q / (p + q);
-            const double pref = TWO_PI_2_5 / (p * q * sqrt(p + q)) * fcd;
+            for (int j = 1; j < Q::KCD; ++j)
+                if (j == kg * Q::KG + i) c = k.c[j];
+            ck[i] = c * fcd;
+        }
+        for (int ib = 0; ib < st.nbp; ++ib) {
+            const double* sb = st.SB + ib * SBW;
+            const double p = sb[0];
+            const double rs = rsqrt(p + q);
+            const double alpha = p * q * rs * rs;
+            const double pref = TWO_PI_2_5 * sb[1] * iq * rs;
             double R[nherm(L)];
-            hermite_r<L>(alpha, Px - __ldg(k + 3), Py - __ldg(k + 4), Pz - __ldg(k + 5), tab, R);
-            double ck[Q::KCD];
-#pragma unroll
-            for (int i = 0; i < Q::KCD; ++i) ck[i] = __ldg(k + 12 + i) * pref;
+            hermite_r<L>(alpha, sb[2] - k.Qx, sb[3] - k.Qy, sb[4] - k.Qz, R);
+            double X[Q::NHB];
 #pragma unroll UH
             for (int t = 0; t <= LAB; ++t)
 #pragma unroll UH
@@ -143,39 +198,33 @@ __device__ __forceinline__ void eri_column(const BraStage& st, const double* __r
                                 }
                             }
                         }
-#pragma unroll
-                        for (int kk = 0; kk < Q::KCD; ++kk) X[hidx(t, u, w)][kk] += ck[kk] * s;
+                        X[hidx(t, u, w)] = pref * s;
                     }
-        }
-        // bra step: v[(ka,kb),ab][kk] += C_bp[ka,kb] f_ab sum_box E^{ab}_tuv X[tuv][kk]
-        const double* E = st.E + (size_t)ib * BE::SIZE;
+            // bra step: v[(ka,kb),ab][kk] += C[ka,kb] f_ab sum_box E^{ab}_tuv X[tuv] ck[kk]
+            const double* E = st.E + (size_t)ib * BE::SIZE;
 #pragma unroll UH
-        for (int ia = 0; ia < Q::NA; ++ia) {
-            const int ax = cart_x(LA, ia), ay = cart_y(LA, ia), az = cart_z(LA, ia);
+            for (int ia = 0; ia < Q::NA; ++ia) {
+                const int ax = cart_x(LA, ia), ay = cart_y(LA, ia), az = cart_z(LA, ia);
 #pragma unroll
-            for (int jb = 0; jb < Q::NB; ++jb) {
-                const int bx = cart_x(LB, jb), by = cart_y(LB, jb), bz = cart_z(LB, jb);
-                const double fab = cart_norm(ax, ay, az) * cart_norm(bx, by, bz);
-                double s[Q::KCD];
+                for (int jb = 0; jb < Q::NB; ++jb) {
+                    const int bx = cart_x(LB, jb), by = cart_y(LB, jb), bz = cart_z(LB, jb);
+                    const double fab = cart_norm(ax, ay, az) * cart_norm(bx, by, bz);
+                    double s = 0.0;
 #pragma unroll
-                for (int kk = 0; kk < Q::KCD; ++kk) s[kk] = 0.0;
+                    for (int t = 0; t <= ax + bx; ++t)
 #pragma unroll
-                for (int t = 0; t <= ax + bx; ++t)
+                        for (int u = 0; u <= ay + by; ++u) {
+                            const double exy = E[BE::at(0, ax, bx, t)] * E[BE::at(1, ay, by, u)];
 #pragma unroll
-                    for (int u = 0; u <= ay + by; ++u) {
-                        const double exy = E[BE::at(0, ax, bx, t)] * E[BE::at(1, ay, by, u)];
-#pragma unroll
-                        for (int w = 0; w <= az + bz; ++w) {
-                            const double e = exy * E[BE::at(2, az, bz, w)];
-#pragma unroll
-                            for (int kk = 0; kk < Q::KCD; ++kk) s[kk] += e * X[hidx(t, u, w)][kk];
+                            for (int w = 0; w <= az + bz; ++w) s += exy * E[BE::at(2, az, bz, w)] * X[hidx(t, u, w)];
                         }
+                    s *= fab;
+#pragma unroll
+                    for (int kab = 0; kab < Q::KAB; ++kab) {
+                        const double c = sb[8 + kab] * s;
+#pragma unroll
+                        for (int kk = 0; kk < Q::KG; ++kk) v[kab * Q::NAB + ia * Q::NB + jb][kk] += c * ck[kk];
                     }
-#pragma unroll
-                for (int kab = 0; kab < Q::KAB; ++kab) {
-                    const double c = b[12 + kab] * fab;
-#pragma unroll
-                    for (int kk = 0; kk < Q::KCD; ++kk) v[kab * Q::NAB + ia * Q::NB + jb][kk] += c * s[kk];
                 }
             }
         }
@@ -186,12 +235,12 @@ __device__ __forceinline__ void eri_column(const BraStage& st, const double* __r
 struct QuartetArgs {
     PairView pv;
     BlockView bv;
-    const double* boys;
     const int* sorted;          // [npair] pair index at sorted position
     const double* sortedQ;      // [npair]
-    const int64_t* counts;      // [NCLS][npair + 1] kept ket prefix length per (ket class, bra position)
+    const int64_t* counts;      // [NSEG][npair + 1] kept ket prefix length per (ket segment, bra position)
+    const int* seg_start;       // [NSEG + 1] sorted position of each segment (device)
     int npair;
-    int cls_start[NCLS + 1];    // sorted positions of each pair class
+    int cls_start[NCLS + 1];    // sorted positions of each angular class (geometry independent)
     int nao;
 };
 
@@ -207,7 +256,8 @@ __device__ __forceinline__ void load_stage(const QuartetArgs& a, int P1, BraStag
     st.nB = a.bv.ncon[st.B];
     st.oA = a.bv.ao[st.A];
     st.oB = a.bv.ao[st.B];
-    st.E = E;
+    st.SB = E;                                   // [nbp][SBW] scalars, then the E tables
+    st.E = E + (size_t)st.nbp * SBW;
 }
 
 struct JKArgs {
@@ -228,8 +278,9 @@ struct JKArgs {
 // A's functions, then B's.
 template <int CX, int CY, int NS>
 __device__ __forceinline__ void jk_digest_column(const JKArgs& a, const BraStage& st, int P2, int C, int Dd, int ic,
-                                                 int id, const double (&v)[QClass<CX, CY>::NROW][QClass<CX, CY>::KCD],
-                                                 double (&jab)[NS][QClass<CX, CY>::NROW], double* Ksm) {
+                                                 int id, int kg,
+                                                 const double (&v)[QClass<CX, CY>::NROW][QClass<CX, CY>::KG],
+                                                 double* Jt, double* Ksm) {
     using Q = QClass<CX, CY>;
     const BlockView& bv = a.q.bv;
     const int nC = bv.ncon[C], nD = bv.ncon[Dd], oC = bv.ao[C], oD = bv.ao[Dd];
@@ -243,11 +294,9 @@ __device__ __forceinline__ void jk_digest_column(const JKArgs& a, const BraStage
         const double* __restrict__ D = a.D + s * nn;
         double* Ks = Ksm + (size_t)s * NF * n;
 #pragma unroll
-        for (int kc = 0; kc < Q::KC; ++kc)
-#pragma unroll
-            for (int kd = 0; kd < Q::KD; ++kd) {
+        for (int kk = 0; kk < Q::KG; ++kk) {
+                const int kq = kg * Q::KG + kk, kc = kq / Q::KD, kd = kq % Q::KD;
                 if (kc >= nC || kd >= nD) continue;
-                const int kk = kc * Q::KD + kd;
                 const int l = oC + kc * Q::NC + ic, sg = oD + kd * Q::ND + id;
                 const double dls = __ldg(D + (size_t)l * n + sg);
                 double jcd = 0.0;
@@ -263,7 +312,7 @@ __device__ __forceinline__ void jk_digest_column(const JKArgs& a, const BraStage
                                 const int r = (ka * Q::KB + kb) * Q::NAB + ia * Q::NB + jb;
                                 const int m = st.oA + ka * Q::NA + ia, nb_ = st.oB + kb * Q::NB + jb;
                                 jcd += v[r][kk] * __ldg(D + (size_t)m * n + nb_);
-                                jab[s][r] += 2.0 * g * v[r][kk] * dls;
+                                Jt[(s * Q::NROW + r) * blockDim.x + threadIdx.x] += 2.0 * g * v[r][kk] * dls;
                             }
                     }
                 atomicAdd(a.J + s * nn + (size_t)l * n + sg, 2.0 * g * jcd);
@@ -315,20 +364,24 @@ __device__ __forceinline__ void jk_digest_column(const JKArgs& a, const BraStage
 
 // Items of ket class CY for the staged bra pair.
 template <int CX, int CY, int NS>
-__device__ __forceinline__ void jk_ket_class(const JKArgs& a, const BraStage& st, int spos,
-                                             double (&jab)[NS][QClass<CX, CY>::NROW], double* Ksm) {
+__device__ __forceinline__ void jk_ket_class(const JKArgs& a, const BraStage& st, int spos, double* Jt, double* Ksm) {
     using Q = QClass<CX, CY>;
-    const int64_t cnt = a.q.counts[(size_t)CY * (a.q.npair + 1) + spos];
-    const int j0 = a.q.cls_start[CY];
-    const int64_t items = cnt * Q::NCD;
-    for (int64_t it = threadIdx.x; it < items; it += blockDim.x) {
-        const int jj = static_cast<int>(it / Q::NCD), cd = static_cast<int>(it % Q::NCD);
-        const int P2 = a.q.sorted[j0 + jj];
-        const int C = a.q.pv.pa_blk[P2], Dd = a.q.pv.pb_blk[P2];
-        const int ic = cd / Q::ND, id = cd % Q::ND;
-        double v[Q::NROW][Q::KCD];
-        eri_column<CX, CY>(st, a.q.pv.rec + a.q.pv.slot[P2] * PPW, a.q.pv.npp[P2], ic, id, a.q.boys, v);
-        jk_digest_column<CX, CY, NS>(a, st, P2, C, Dd, ic, id, v, jab, Ksm);
+    for (int sub = 0; sub < NSUB; ++sub) {
+        const int seg = CY * NSUB + sub;
+        const int64_t cnt = a.q.counts[(size_t)seg * (a.q.npair + 1) + spos];
+        if (cnt == 0) continue;
+        const int j0 = a.q.seg_start[seg];
+        const int64_t items = cnt * Q::NCD * Q::NKG;
+        for (int64_t it = threadIdx.x; it < items; it += blockDim.x) {
+            const int kg = static_cast<int>(it % Q::NKG);
+            const int jj = static_cast<int>(it / (Q::NCD * Q::NKG)), cd = static_cast<int>((it / Q::NKG) % Q::NCD);
+            const int P2 = a.q.sorted[j0 + jj];
+            const int C = a.q.pv.pa_blk[P2], Dd = a.q.pv.pb_blk[P2];
+            const int ic = cd / Q::ND, id = cd % Q::ND;
+            double v[Q::NROW][Q::KG];
+            eri_column<CX, CY>(st, a.q.pv.rec + a.q.pv.slot[P2] * PPW, a.q.pv.npp[P2], ic, id, kg, v);
+            jk_digest_column<CX, CY, NS>(a, st, P2, C, Dd, ic, id, kg, v, Jt, Ksm);
+        }
     }
 }
 
@@ -340,45 +393,39 @@ struct JKKernel {
     static constexpr int ESIZE = BraE<Q0::LA, Q0::LB, 0>::SIZE;
 };
 
-// Dynamic shared memory: K rows [NS][NF][nao], J_ab [NS][NROW], bra E tables.
+// Dynamic shared memory: K rows [NS][NF][nao], per-thread J_ab slots
+// [NS][NROW][blockDim], bra E tables.
+constexpr int JK_THREADS = 128;
+
 template <int CX, int NS>
-__global__ void __launch_bounds__(128) jk_bra_kernel(JKArgs a) {
+__global__ void __launch_bounds__(JK_THREADS) jk_bra_kernel(JKArgs a) {
     using KK = JKKernel<CX, NS>;
     using Q0 = QClass<CX, 0>;
     extern __shared__ double smem[];
     const int n = a.q.nao;
     double* Ksm = smem;
-    double* Jsm = Ksm + (size_t)NS * KK::NF * n;
-    double* Esm = Jsm + NS * KK::NROW;
+    double* Jt = Ksm + (size_t)NS * KK::NF * n;
+    double* Esm = Jt + NS * KK::NROW * JK_THREADS;
     const int spos = a.q.cls_start[CX] + blockIdx.x;
     const int P1 = a.q.sorted[spos];
     __shared__ BraStage st;
     if (threadIdx.x == 0) load_stage(a.q, P1, st, Esm);
-    for (int i = threadIdx.x; i < NS * KK::NF * n + NS * KK::NROW; i += blockDim.x) smem[i] = 0.0;
+    for (int i = threadIdx.x; i < NS * KK::NF * n + NS * KK::NROW * JK_THREADS; i += blockDim.x) smem[i] = 0.0;
     __syncthreads();
     stage_bra_e<Q0::LA, Q0::LB, 0>(st);
     __syncthreads();
-    double jab[NS][KK::NROW];
-#pragma unroll
-    for (int s = 0; s < NS; ++s)
-#pragma unroll
-        for (int r = 0; r < KK::NROW; ++r) jab[s][r] = 0.0;
-    if (CX >= 0) jk_ket_class<CX, 0, NS>(a, st, spos, jab, Ksm);
-    if constexpr (CX >= 1) jk_ket_class<CX, 1, NS>(a, st, spos, jab, Ksm);
-    if constexpr (CX >= 2) jk_ket_class<CX, 2, NS>(a, st, spos, jab, Ksm);
-    if constexpr (CX >= 3) jk_ket_class<CX, 3, NS>(a, st, spos, jab, Ksm);
-    if constexpr (CX >= 4) jk_ket_class<CX, 4, NS>(a, st, spos, jab, Ksm);
-    if constexpr (CX >= 5) jk_ket_class<CX, 5, NS>(a, st, spos, jab, Ksm);
-#pragma unroll
-    for (int s = 0; s < NS; ++s)
-#pragma unroll
-        for (int r = 0; r < KK::NROW; ++r)
-            if (jab[s][r] != 0.0) atomicAdd(Jsm + s * KK::NROW + r, jab[s][r]);
+    jk_ket_class<CX, 0, NS>(a, st, spos, Jt, Ksm);
+    if constexpr (CX >= 1) jk_ket_class<CX, 1, NS>(a, st, spos, Jt, Ksm);
+    if constexpr (CX >= 2) jk_ket_class<CX, 2, NS>(a, st, spos, Jt, Ksm);
+    if constexpr (CX >= 3) jk_ket_class<CX, 3, NS>(a, st, spos, Jt, Ksm);
+    if constexpr (CX >= 4) jk_ket_class<CX, 4, NS>(a, st, spos, Jt, Ksm);
+    if constexpr (CX >= 5) jk_ket_class<CX, 5, NS>(a, st, spos, Jt, Ksm);
     __syncthreads();
     const size_t nn = (size_t)n * n;
-    // flush J_ab
+    // flush J_ab: one thread per (set, row) sums the per-thread slots
     for (int i = threadIdx.x; i < NS * KK::NROW; i += blockDim.x) {
-        const double val = Jsm[i];
+        double val = 0.0;
+        for (int t = 0; t < JK_THREADS; ++t) val += Jt[i * JK_THREADS + t];
         if (val == 0.0) continue;
         const int s = i / KK::NROW, r = i % KK::NROW;
         const int kab = r / Q0::NAB, ab = r % Q0::NAB;
@@ -392,8 +439,7 @@ __global__ void __launch_bounds__(128) jk_bra_kernel(JKArgs a) {
         const double val = Ksm[i];
         if (val == 0.0) continue;
         const int col = i % n, f = (i / n) % KK::NF, s = i / (n * KK::NF);
-        const int row = f < NFA ? st.oA + (f / Q0::NA) * Q0::NA + f % Q0::NA
-                                : st.oB + ((f - NFA) / Q0::NB) * Q0::NB + (f - NFA) % Q0::NB;
+        const int row = f < NFA ? st.oA + f : st.oB + (f - NFA);
         atomicAdd(a.K + s * nn + (size_t)row * n + col, val);
     }
 }
@@ -401,7 +447,8 @@ __global__ void __launch_bounds__(128) jk_bra_kernel(JKArgs a) {
 template <int CX, int NS>
 size_t jk_smem_bytes(int nao, int max_bra_prims) {
     using KK = JKKernel<CX, NS>;
-    return sizeof(double) * ((size_t)NS * KK::NF * nao + NS * KK::NROW + (size_t)max_bra_prims * KK::ESIZE);
+    return sizeof(double) * ((size_t)NS * KK::NF * nao + (size_t)NS * KK::NROW * JK_THREADS +
+                             (size_t)max_bra_prims * (KK::ESIZE + SBW));
 }
 
 // ---------------------------------------------------------- Schwarz
@@ -423,8 +470,9 @@ __global__ void __launch_bounds__(64) schwarz_kernel(QuartetArgs a, const int* p
     stage_bra_e<Q::LA, Q::LB, 0>(st);
     __syncthreads();
     for (int cd = threadIdx.x; cd < Q::NCD; cd += blockDim.x) {
+        static_assert(Q::KG == Q::KCD, "diagonal quartets keep all contraction combinations in one item");
         double v[Q::NROW][Q::KCD];
-        eri_column<CX, CX>(st, st.rec, st.nbp, cd / Q::ND, cd % Q::ND, a.boys, v);
+        eri_column<CX, CX>(st, st.rec, st.nbp, cd / Q::ND, cd % Q::ND, 0, v);
         double m = 0.0;
 #pragma unroll
         for (int ka = 0; ka < Q::KA; ++ka)

@@ -29,11 +29,30 @@ struct GradArgs {
     int natm;
 };
 
+// For runtime (i, j): row[t] = E^{ij}_t and drow[t] = 2c E^{i+1,j}_t - i E^{i-1,j}_t
+// (the d/dC_x expansion), selected by predicated copies.
+template <int LC, int LD>
+__device__ __forceinline__ void ket_deriv_rows(const double (&e)[LC + 2][LD + 1][LC + LD + 2], int i, int j, double c,
+                                               double (&row)[LC + LD + 2], double (&drow)[LC + LD + 2]) {
+#pragma unroll
+    for (int t = 0; t <= LC + LD + 1; ++t) row[t] = drow[t] = 0.0;
+#pragma unroll
+    for (int ii = 0; ii <= LC; ++ii)
+#pragma unroll
+        for (int jj = 0; jj <= LD; ++jj)
+            if (ii == i && jj == j)
+#pragma unroll
+                for (int t = 0; t <= LC + LD + 1; ++t) {
+                    row[t] = t <= LC + LD ? e[ii][jj][t] : 0.0;
+                    drow[t] = 2.0 * c * e[ii + 1][jj][t] - (ii > 0 ? ii * e[ii > 0 ? ii - 1 : 0][jj][t] : 0.0);
+                }
+}
+
 // Gradient contribution of one column; adds A, B parts to gab and C, D
 // parts to the shared accumulator gsh[natm][3].
 template <int CX, int CY>
 __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStage& st, int P2, double QQ, int ic,
-                                            int id, double (&gab)[6], double* gsh) {
+                                            int id, int kg, double (&gab)[6], double* gsh) {
     using Q = QClass<CX, CY>;
     using BE = BraE<Q::LA, Q::LB, 1>;
     constexpr int LA = Q::LA, LB = Q::LB, LC = Q::LC, LD = Q::LD, LAB = Q::LAB, LCD = Q::LCD, L = Q::L + 1;
@@ -49,11 +68,11 @@ __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStage& s
     const size_t nn = (size_t)n * n;
     const double deg = 0.5 * (st.A != st.B ? 2.0 : 1.0) * (C != Dd ? 2.0 : 1.0) * (st.P1 != P2 ? 2.0 : 1.0);
     // Gamma column
-    double G[Q::NROW][Q::KCD];
+    double G[Q::NROW][Q::KG];
     double gmax = 0.0;
 #pragma unroll
-    for (int kk = 0; kk < Q::KCD; ++kk) {
-        const int kc = kk / Q::KD, kd = kk % Q::KD;
+    for (int kk = 0; kk < Q::KG; ++kk) {
+        const int kq = kg * Q::KG + kk, kc = kq / Q::KD, kd = kq % Q::KD;
         const bool cv = kc < nC && kd < nD;
         const size_t l = oC + kc * Q::NC + ic, sg = oD + kd * Q::ND + id;
 #pragma unroll
@@ -81,84 +100,58 @@ __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStage& s
     const double fcd = cart_norm(cx, cy, cz) * cart_norm(dx, dy, dz);
     const double* rk = a.q.pv.rec + a.q.pv.slot[P2] * PPW;
     const int nkp = a.q.pv.npp[P2];
-    for (int ib = 0; ib < st.nbp; ++ib) {
-        const double* b = st.rec + (size_t)ib * PPW;
-        const double ea = b[0], eb = b[1], p = ea + eb;
-        const double* E = st.E + (size_t)ib * BE::SIZE;
-        // Gamma contracted with this bra primitive's coefficients (and f_ab),
-        // and its bra Hermite transform Y[h][kk] (for the C-centre pass)
-        double gb[Q::NAB][Q::KCD];
-        double Y[Q::NHB][Q::KCD];
+    for (int ik = 0; ik < nkp; ++ik) {
+        const KetRec k = load_ket(rk + (size_t)ik * PPW);
+        const double ec = k.a, q = ec + k.b, oo2q = 0.5 / q, iq = 2.0 * oo2q;
+        // ket E for this column, and d/dC_d of it (one extra in direction d)
+        double ex[LCD + 2], ey[LCD + 2], ez[LCD + 2], gx[LCD + 2], gy[LCD + 2], gz[LCD + 2];
+        {
+            double e[LC + 2][LD + 1][LCD + 2];
+            hermite_e<LC + 1, LD>(k.QAx, k.QBx, oo2q, k.K, e);
+            ket_deriv_rows<LC, LD>(e, cx, dx, ec, ex, gx);
+            hermite_e<LC + 1, LD>(k.QAy, k.QBy, oo2q, 1.0, e);
+            ket_deriv_rows<LC, LD>(e, cy, dy, ec, ey, gy);
+            hermite_e<LC + 1, LD>(k.QAz, k.QBz, oo2q, 1.0, e);
+            ket_deriv_rows<LC, LD>(e, cz, dz, ec, ez, gz);
+        }
+        double ck[Q::KG];
 #pragma unroll
-        for (int h = 0; h < Q::NHB; ++h)
+        for (int i = 0; i < Q::KG; ++i) {
+            double c = k.c[0];
 #pragma unroll
-            for (int kk = 0; kk < Q::KCD; ++kk) Y[h][kk] = 0.0;
-#pragma unroll UH
-        for (int ia = 0; ia < Q::NA; ++ia) {
-            const int ax = cart_x(LA, ia), ay = cart_y(LA, ia), az = cart_z(LA, ia);
+            for (int j = 1; j < Q::KCD; ++j)
+                if (j == kg * Q::KG + i) c = k.c[j];
+            ck[i] = c * fcd;
+        }
+        for (int ib = 0; ib < st.nbp; ++ib) {
+            const double* sb = st.SB + ib * SBW;
+            const double p = sb[0], ea = sb[5], eb = sb[6];
+            const double rs = rsqrt(p + q);
+            const double alpha = p * q * rs * rs;
+            const double pref = TWO_PI_2_5 * sb[1] * iq * rs;
+            const double* E = st.E + (size_t)ib * BE::SIZE;
+            double R[nherm(L)];
+            hermite_r<L>(alpha, sb[2] - k.Qx, sb[3] - k.Qy, sb[4] - k.Qz, R);
+            // Gamma contracted with this bra primitive's coefficients and f_ab,
+            // then summed over the ket contractions: gq[ab] = sum_kk gb[ab][kk] ck[kk]
+            double gq[Q::NAB];
 #pragma unroll
-            for (int jb = 0; jb < Q::NB; ++jb) {
-                const int bx = cart_x(LB, jb), by = cart_y(LB, jb), bz = cart_z(LB, jb);
-                const double fab = cart_norm(ax, ay, az) * cart_norm(bx, by, bz);
-                const int ab = ia * Q::NB + jb;
+            for (int ia = 0; ia < Q::NA; ++ia)
 #pragma unroll
-                for (int kk = 0; kk < Q::KCD; ++kk) {
+                for (int jb = 0; jb < Q::NB; ++jb) {
+                    const double fab = cart_norm(cart_x(LA, ia), cart_y(LA, ia), cart_z(LA, ia)) *
+                                       cart_norm(cart_x(LB, jb), cart_y(LB, jb), cart_z(LB, jb));
+                    const int ab = ia * Q::NB + jb;
                     double s = 0.0;
 #pragma unroll
-                    for (int kab = 0; kab < Q::KAB; ++kab) s += b[12 + kab] * G[kab * Q::NAB + ab][kk];
-                    gb[ab][kk] = s * fab;
+                    for (int kab = 0; kab < Q::KAB; ++kab)
+#pragma unroll
+                        for (int kk = 0; kk < Q::KG; ++kk) s += sb[8 + kab] * G[kab * Q::NAB + ab][kk] * ck[kk];
+                    gq[ab] = s * fab * pref;
                 }
-#pragma unroll
-                for (int t = 0; t <= ax + bx; ++t)
-#pragma unroll
-                    for (int u = 0; u <= ay + by; ++u)
-#pragma unroll
-                        for (int w = 0; w <= az + bz; ++w) {
-                            const double e = E[BE::at(0, ax, bx, t)] * E[BE::at(1, ay, by, u)] * E[BE::at(2, az, bz, w)];
-#pragma unroll
-                            for (int kk = 0; kk < Q::KCD; ++kk) Y[hidx(t, u, w)][kk] += e * gb[ab][kk];
-                        }
-            }
-        }
-        double Xb[NH1][Q::KCD];
-#pragma unroll
-        for (int h = 0; h < NH1; ++h)
-#pragma unroll
-            for (int kk = 0; kk < Q::KCD; ++kk) Xb[h][kk] = 0.0;
-        for (int ik = 0; ik < nkp; ++ik) {
-            const double* k = rk + (size_t)ik * PPW;
-            const double ec = __ldg(k), q = ec + __ldg(k + 1), oo2q = 0.5 / q;
-            // ket E for this column, and d/dC_d of it (one extra in direction d)
-            double ex[LCD + 2], ey[LCD + 2], ez[LCD + 2], gx[LCD + 2], gy[LCD + 2], gz[LCD + 2];
-            {
-                double e[LC + 2][LD + 1][LCD + 2];
-                hermite_e<LC + 1, LD>(__ldg(k + 6), __ldg(k + 9), oo2q, __ldg(k + 2), e);
-#pragma unroll
-                for (int t = 0; t <= LCD + 1; ++t) {
-                    ex[t] = t <= LCD ? e[cx][dx][t] : 0.0;
-                    gx[t] = 2.0 * ec * e[cx + 1][dx][t] - (cx > 0 ? cx * e[cx > 0 ? cx - 1 : 0][dx][t] : 0.0);
-                }
-                hermite_e<LC + 1, LD>(__ldg(k + 7), __ldg(k + 10), oo2q, 1.0, e);
-#pragma unroll
-                for (int t = 0; t <= LCD + 1; ++t) {
-                    ey[t] = t <= LCD ? e[cy][dy][t] : 0.0;
-                    gy[t] = 2.0 * ec * e[cy + 1][dy][t] - (cy > 0 ? cy * e[cy > 0 ? cy - 1 : 0][dy][t] : 0.0);
-                }
-                hermite_e<LC + 1, LD>(__ldg(k + 8), __ldg(k + 11), oo2q, 1.0, e);
-#pragma unroll
-                for (int t = 0; t <= LCD + 1; ++t) {
-                    ez[t] = t <= LCD ? e[cz][dz][t] : 0.0;
-                    gz[t] = 2.0 * ec * e[cz + 1][dz][t] - (cz > 0 ? cz * e[cz > 0 ? cz - 1 : 0][dz][t] : 0.0);
-                }
-            }
-            const double alpha = p * q / (p + q);
-            const double pref = TWO_PI_2_5 / (p * q * sqrt(p + q)) * fcd;
-            double R[nherm(L)];
-            hermite_r<L>(alpha, b[3] - __ldg(k + 3), b[4] - __ldg(k + 4), b[5] - __ldg(k + 5), a.q.boys, R);
-            double ck[Q::KCD];
-#pragma unroll
-            for (int i = 0; i < Q::KCD; ++i) ck[i] = __ldg(k + 12 + i) * pref;
-            // bra pass: Xb[h][kk] += sum_{k in box(cd)} (-1)^|k| E^{cd}_k R_{h+k} ck
+            // bra pass (A, B): sum_ab gq[ab] sum_{h in dbox(ab)} dE_h Xb_h,
+            // Xb_h = sum_{k in box(cd)} (-1)^|k| E^{cd}_k R_{h+k}
+            double Xb[NH1];
 #pragma unroll UH
             for (int t = 0; t <= LAB + 1; ++t)
 #pragma unroll UH
@@ -180,19 +173,54 @@ __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStage& s
                                 }
                             }
                         }
-#pragma unroll
-                        for (int kk = 0; kk < Q::KCD; ++kk) Xb[hidx(t, u, w)][kk] += ck[kk] * s;
+                        Xb[hidx(t, u, w)] = s;
                     }
-            // C-centre pass: dC_d += sum_h sum_k (-1)^|k| dE^{cd}_{d,k} R_{h+k} (sum_kk Y[h][kk] ck[kk])
+            // C pass: Y_h = sum_ab gq[ab] E^{ab}_h (h <= LAB), then
+            // dC_d += sum_h Y_h sum_k (-1)^|k| dE^{cd}_{d,k} R_{h+k}
+            double Y[Q::NHB];
+#pragma unroll
+            for (int h = 0; h < Q::NHB; ++h) Y[h] = 0.0;
+#pragma unroll UH
+            for (int ia = 0; ia < Q::NA; ++ia) {
+                const int ax = cart_x(LA, ia), ay = cart_y(LA, ia), az = cart_z(LA, ia);
+#pragma unroll
+                for (int jb = 0; jb < Q::NB; ++jb) {
+                    const int bx = cart_x(LB, jb), by = cart_y(LB, jb), bz = cart_z(LB, jb);
+                    const double g = gq[ia * Q::NB + jb];
+#pragma unroll
+                    for (int t = 0; t <= ax + bx + 1; ++t)
+#pragma unroll
+                        for (int u = 0; u <= ay + by + 1; ++u)
+#pragma unroll
+                            for (int w = 0; w <= az + bz + 1; ++w) {
+                                const int over = (t > ax + bx) + (u > ay + by) + (w > az + bz);
+                                if (over > 1) continue;
+                                const double yv = g * Xb[hidx(t, u, w)];
+                                const double e0 = E[BE::at(0, ax, bx, t)], e1 = E[BE::at(1, ay, by, u)],
+                                             e2 = E[BE::at(2, az, bz, w)];
+                                if (over == 0) Y[hidx(t, u, w)] += g * e0 * e1 * e2;
+                                const double dax = 2.0 * ea * E[BE::at(0, ax + 1, bx, t)] - (ax > 0 ? ax * E[BE::at(0, ax > 0 ? ax - 1 : 0, bx, t)] : 0.0);
+                                const double day = 2.0 * ea * E[BE::at(1, ay + 1, by, u)] - (ay > 0 ? ay * E[BE::at(1, ay > 0 ? ay - 1 : 0, by, u)] : 0.0);
+                                const double daz = 2.0 * ea * E[BE::at(2, az + 1, bz, w)] - (az > 0 ? az * E[BE::at(2, az > 0 ? az - 1 : 0, bz, w)] : 0.0);
+                                const double dbx = 2.0 * eb * E[BE::at(0, ax, bx + 1, t)] - (bx > 0 ? bx * E[BE::at(0, ax, bx > 0 ? bx - 1 : 0, t)] : 0.0);
+                                const double dby = 2.0 * eb * E[BE::at(1, ay, by + 1, u)] - (by > 0 ? by * E[BE::at(1, ay, by > 0 ? by - 1 : 0, u)] : 0.0);
+                                const double dbz = 2.0 * eb * E[BE::at(2, az, bz + 1, w)] - (bz > 0 ? bz * E[BE::at(2, az, bz > 0 ? bz - 1 : 0, w)] : 0.0);
+                                dA[0] += yv * dax * e1 * e2;
+                                dA[1] += yv * e0 * day * e2;
+                                dA[2] += yv * e0 * e1 * daz;
+                                dB[0] += yv * dbx * e1 * e2;
+                                dB[1] += yv * e0 * dby * e2;
+                                dB[2] += yv * e0 * e1 * dbz;
+                            }
+                }
+            }
 #pragma unroll UH
             for (int t = 0; t <= LAB; ++t)
 #pragma unroll UH
                 for (int u = 0; u <= LAB - t; ++u)
 #pragma unroll UW
                     for (int w = 0; w <= LAB - t - u; ++w) {
-                        double yv = 0.0;
-#pragma unroll
-                        for (int kk = 0; kk < Q::KCD; ++kk) yv += Y[hidx(t, u, w)][kk] * ck[kk];
+                        const double yv = Y[hidx(t, u, w)];
                         double s0 = 0.0, s1 = 0.0, s2 = 0.0;
 #pragma unroll
                         for (int t2 = 0; t2 <= LCD + 1; ++t2) {
@@ -218,42 +246,6 @@ __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStage& s
                         dC[2] += yv * s2;
                     }
         }
-        // bra pass, A and B: sum_ab sum_kk gb[ab][kk] sum_{h in dbox(ab)} dE_h Xb[h][kk]
-#pragma unroll UH
-        for (int ia = 0; ia < Q::NA; ++ia) {
-            const int ax = cart_x(LA, ia), ay = cart_y(LA, ia), az = cart_z(LA, ia);
-#pragma unroll
-            for (int jb = 0; jb < Q::NB; ++jb) {
-                const int bx = cart_x(LB, jb), by = cart_y(LB, jb), bz = cart_z(LB, jb);
-                const int ab = ia * Q::NB + jb;
-#pragma unroll
-                for (int t = 0; t <= ax + bx + 1; ++t)
-#pragma unroll
-                    for (int u = 0; u <= ay + by + 1; ++u)
-#pragma unroll
-                        for (int w = 0; w <= az + bz + 1; ++w) {
-                            const int over = (t > ax + bx) + (u > ay + by) + (w > az + bz);
-                            if (over > 1) continue;
-                            double yv = 0.0;
-#pragma unroll
-                            for (int kk = 0; kk < Q::KCD; ++kk) yv += gb[ab][kk] * Xb[hidx(t, u, w)][kk];
-                            const double e0 = E[BE::at(0, ax, bx, t)], e1 = E[BE::at(1, ay, by, u)],
-                                         e2 = E[BE::at(2, az, bz, w)];
-                            const double dax = 2.0 * ea * E[BE::at(0, ax + 1, bx, t)] - (ax > 0 ? ax * E[BE::at(0, ax > 0 ? ax - 1 : 0, bx, t)] : 0.0);
-                            const double day = 2.0 * ea * E[BE::at(1, ay + 1, by, u)] - (ay > 0 ? ay * E[BE::at(1, ay > 0 ? ay - 1 : 0, by, u)] : 0.0);
-                            const double daz = 2.0 * ea * E[BE::at(2, az + 1, bz, w)] - (az > 0 ? az * E[BE::at(2, az > 0 ? az - 1 : 0, bz, w)] : 0.0);
-                            const double dbx = 2.0 * eb * E[BE::at(0, ax, bx + 1, t)] - (bx > 0 ? bx * E[BE::at(0, ax, bx > 0 ? bx - 1 : 0, t)] : 0.0);
-                            const double dby = 2.0 * eb * E[BE::at(1, ay, by + 1, u)] - (by > 0 ? by * E[BE::at(1, ay, by > 0 ? by - 1 : 0, u)] : 0.0);
-                            const double dbz = 2.0 * eb * E[BE::at(2, az, bz + 1, w)] - (bz > 0 ? bz * E[BE::at(2, az, bz > 0 ? bz - 1 : 0, w)] : 0.0);
-                            dA[0] += yv * dax * e1 * e2;
-                            dA[1] += yv * e0 * day * e2;
-                            dA[2] += yv * e0 * e1 * daz;
-                            dB[0] += yv * dbx * e1 * e2;
-                            dB[1] += yv * e0 * dby * e2;
-                            dB[2] += yv * e0 * e1 * dbz;
-                        }
-            }
-        }
     }
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
@@ -268,37 +260,46 @@ template <int CX, int CY>
 __device__ __forceinline__ void grad_ket_class(const GradArgs& a, const BraStage& st, int spos, double (&gab)[6],
                                                double* gsh) {
     using Q = QClass<CX, CY>;
-    const int64_t cnt = a.q.counts[(size_t)CY * (a.q.npair + 1) + spos];
-    const int j0 = a.q.cls_start[CY];
     const double q1 = a.q.sortedQ[spos];
-    for (int64_t it = threadIdx.x; it < cnt * Q::NCD; it += blockDim.x) {
-        const int jj = static_cast<int>(it / Q::NCD), cd = static_cast<int>(it % Q::NCD);
-        const int P2 = a.q.sorted[j0 + jj];
-        grad_column<CX, CY>(a, st, P2, q1 * a.q.sortedQ[j0 + jj], cd / Q::ND, cd % Q::ND, gab, gsh);
+    for (int sub = 0; sub < NSUB; ++sub) {
+        const int seg = CY * NSUB + sub;
+        const int64_t cnt = a.q.counts[(size_t)seg * (a.q.npair + 1) + spos];
+        if (cnt == 0) continue;
+        const int j0 = a.q.seg_start[seg];
+        for (int64_t it = threadIdx.x; it < cnt * Q::NCD * Q::NKG; it += blockDim.x) {
+            const int kg = static_cast<int>(it % Q::NKG);
+            const int jj = static_cast<int>(it / (Q::NCD * Q::NKG)), cd = static_cast<int>((it / Q::NKG) % Q::NCD);
+            const int P2 = a.q.sorted[j0 + jj];
+            grad_column<CX, CY>(a, st, P2, q1 * a.q.sortedQ[j0 + jj], cd / Q::ND, cd % Q::ND, kg, gab, gsh);
+        }
     }
 }
 
-// Dynamic shared memory: gradient accumulator [natm][3], bra E tables (+1).
-template <int CX>
+// One kernel per (bra class, ket class): CTA per bra pair of class CX, items
+// over the ket segments of class CY. Dynamic shared memory: gradient
+// accumulator [natm][3], bra E tables (+1).
+template <int CX, int CY>
 __global__ void __launch_bounds__(128) grad2e_bra_kernel(GradArgs a) {
     using Q0 = QClass<CX, 0>;
     extern __shared__ double smem[];
     double* gsh = smem;
     double* Esm = smem + 3 * a.natm;
     __shared__ BraStage st;
+    __shared__ int any;
     const int spos = a.q.cls_start[CX] + blockIdx.x;
-    if (threadIdx.x == 0) load_stage(a.q, a.q.sorted[spos], st, Esm);
-    for (int i = threadIdx.x; i < 3 * a.natm; i += blockDim.x) gsh[i] = 0.0;
+    if (threadIdx.x == 0) {
+        load_stage(a.q, a.q.sorted[spos], st, Esm);
+        int64_t tot = 0;
+        for (int sub = 0; sub < NSUB; ++sub) tot += a.q.counts[(size_t)(CY * NSUB + sub) * (a.q.npair + 1) + spos];
+        any = tot > 0;
+    }
     __syncthreads();
+    if (!any) return;
+    for (int i = threadIdx.x; i < 3 * a.natm; i += blockDim.x) gsh[i] = 0.0;
     stage_bra_e<Q0::LA, Q0::LB, 1>(st);
     __syncthreads();
     double gab[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    grad_ket_class<CX, 0>(a, st, spos, gab, gsh);
-    if constexpr (CX >= 1) grad_ket_class<CX, 1>(a, st, spos, gab, gsh);
-    if constexpr (CX >= 2) grad_ket_class<CX, 2>(a, st, spos, gab, gsh);
-    if constexpr (CX >= 3) grad_ket_class<CX, 3>(a, st, spos, gab, gsh);
-    if constexpr (CX >= 4) grad_ket_class<CX, 4>(a, st, spos, gab, gsh);
-    if constexpr (CX >= 5) grad_ket_class<CX, 5>(a, st, spos, gab, gsh);
+    grad_ket_class<CX, CY>(a, st, spos, gab, gsh);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         if (gab[d] != 0.0) atomicAdd(gsh + 3 * st.aA + d, gab[d]);
@@ -312,7 +313,7 @@ __global__ void __launch_bounds__(128) grad2e_bra_kernel(GradArgs a) {
 template <int CX>
 size_t grad_smem_bytes(int natm, int max_bra_prims) {
     using Q0 = QClass<CX, 0>;
-    return sizeof(double) * (3 * (size_t)natm + (size_t)max_bra_prims * BraE<Q0::LA, Q0::LB, 1>::SIZE);
+    return sizeof(double) * (3 * (size_t)natm + (size_t)max_bra_prims * (BraE<Q0::LA, Q0::LB, 1>::SIZE + SBW));
 }
 
 }  // namespace hf

@@ -32,27 +32,6 @@ namespace {
 
 thread_local char g_err[512] = "";
 
-// Boys table F_n(0.1 k), n < BOYS_COLS: the positive series for a high order
-// (all terms positive, no cancellation), then downward recursion.
-std::vector<double> boys_table() {
-    const int top = 32;
-    std::vector<double> t(BOYS_NGRID * BOYS_COLS);
-    std::vector<double> col(top + 1);
-    for (int k = 0; k < BOYS_NGRID; ++k) {
-        const double x = 0.1 * k;
-        double term = 1.0 / (2 * top + 1), total = term;
-        for (int j = 1; j < 400; ++j) {
-            term = term * (2.0 * x) / (2 * top + 2 * j + 1);
-            total += term;
-        }
-        const double ex = std::exp(-x);
-        col[top] = ex * total;
-        for (int n = top - 1; n >= 0; --n) col[n] = (2.0 * x * col[n + 1] + ex) / (2 * n + 1);
-        for (int n = 0; n < BOYS_COLS; ++n) t[k * BOYS_COLS + n] = col[n];
-    }
-    return t;
-}
-
 template <typename T>
 cudaError_t dalloc(T** p, size_t n) { return cudaMalloc(reinterpret_cast<void**>(p), std::max<size_t>(n, 1) * sizeof(T)); }
 
@@ -76,17 +55,23 @@ struct aimd_ctx {
     double* Q;
     int cls_start[NCLS + 1];
     int* by_class;          // pair indices grouped by class (static)
-    int* seg_begin;         // cub segment offsets
-    double* keys_in;
+    int* idx_in;            // 0..npair-1
+    int* tmp_idx;           // pair order after the Q sort
+    int* seg_id;            // segment of each pair (geometry dependent)
+    int* seg_keys;          // segment of each Q-sorted position
+    int* seg_keys_out;
+    int* seg_start;         // [NSEG + 1] (device)
+    double* tmpQ;
     double* sortedQ;
     int* sorted;
-    int64_t* counts_jk;     // [NCLS][npair + 1] kept ket prefix per (ket class, bra position)
+    int64_t* counts_jk;     // [NSEG][npair + 1] kept ket prefix per (ket segment, bra position)
     int64_t* counts_g;
+    cudaStream_t cls_stream[NCLS];
+    cudaEvent_t ev_fork, ev_join[NCLS];
     int maxbp[NCLS];        // largest primitive-pair count of a block pair, per class
     double thr_jk = -1.0, thr_g = -1.0;
     void* cub_tmp;
     size_t cub_bytes;
-    double* boys;
     double* pos;            // [natm][3] device copy of the current geometry
     bool have_geometry = false;
     uint64_t launches = 0;
@@ -148,10 +133,6 @@ extern "C" int aimd_create(aimd_ctx** out, int natm, int nao, int nblock, const 
     CK(up_d(&c->sh_exp, sh_exp, nsprim));
     CK(up_d(&c->sh_coef, sh_coef, nsprim));
     CK(up_d(&c->charges, charges, natm));
-    {   // Boys table
-        std::vector<double> t = boys_table();
-        CK(up_d(&c->boys, t.data(), t.size()));
-    }
     CK(dalloc(&c->pos, 3 * (size_t)natm));
     // shell pairs (si >= sj) grouped by class (l_i >= l_j after orientation)
     {
@@ -201,30 +182,41 @@ extern "C" int aimd_create(aimd_ctx** out, int natm, int nao, int nblock, const 
                 if (cls[p] == cl) by.push_back(p);
         }
         c->cls_start[NCLS] = np;
-        std::vector<int> seg(c->cls_start, c->cls_start + NCLS + 1);
+        std::vector<int> iota(np);
+        for (int p = 0; p < np; ++p) iota[p] = p;
         CK(up_i(&c->pa, pa.data(), np));
         CK(up_i(&c->pb, pb.data(), np));
         CK(up_i(&c->by_class, by.data(), np));
-        CK(up_i(&c->seg_begin, seg.data(), NCLS + 1));
+        CK(up_i(&c->idx_in, iota.data(), np));
+        CK(dalloc(&c->tmp_idx, np));
+        CK(dalloc(&c->seg_id, np));
+        CK(dalloc(&c->seg_keys, np));
+        CK(dalloc(&c->seg_keys_out, np));
+        CK(dalloc(&c->seg_start, NSEG + 1));
+        CK(dalloc(&c->tmpQ, np));
         CK(dalloc(&c->slot, np));
         CK(cudaMemcpy(c->slot, slot.data(), np * sizeof(int64_t), cudaMemcpyHostToDevice));
         CK(dalloc(&c->npp, np));
         CK(dalloc(&c->rec, (size_t)nrec * PPW));
         CK(dalloc(&c->Q, np));
-        CK(dalloc(&c->keys_in, np));
         CK(dalloc(&c->sortedQ, np));
         CK(dalloc(&c->sorted, np));
-        CK(dalloc(&c->counts_jk, (size_t)NCLS * (np + 1)));
-        CK(dalloc(&c->counts_g, (size_t)NCLS * (np + 1)));
+        CK(dalloc(&c->counts_jk, (size_t)NSEG * (np + 1)));
+        CK(dalloc(&c->counts_g, (size_t)NSEG * (np + 1)));
         for (int cl = 0; cl < NCLS; ++cl) c->maxbp[cl] = 1;
         for (int p = 0; p < np; ++p)
             c->maxbp[cls[p]] = std::max(c->maxbp[cls[p]], blk_np[pa[p]] * blk_np[pb[p]]);
-        size_t b1 = 0;
-        CK(cub::DeviceSegmentedRadixSort::SortPairsDescending(nullptr, b1, c->keys_in, c->sortedQ, c->by_class,
-                                                               c->sorted, np, NCLS, c->seg_begin, c->seg_begin + 1));
-        c->cub_bytes = b1;
+        size_t b1 = 0, b2 = 0;
+        CK(cub::DeviceRadixSort::SortPairsDescending(nullptr, b1, c->Q, c->tmpQ, c->idx_in, c->tmp_idx, np));
+        CK(cub::DeviceRadixSort::SortPairs(nullptr, b2, c->seg_keys, c->seg_keys_out, c->tmp_idx, c->sorted, np));
+        c->cub_bytes = std::max(b1, b2);
         CK(cudaMalloc(&c->cub_tmp, c->cub_bytes));
     }
+    for (int i = 0; i < NCLS; ++i) {
+        CK(cudaStreamCreateWithFlags(&c->cls_stream[i], cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&c->ev_join[i], cudaEventDisableTiming));
+    }
+    CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
     *out = c;
     return AIMD_OK;
 }
@@ -233,9 +225,15 @@ extern "C" int aimd_destroy(aimd_ctx* c) {
     if (!c) return AIMD_OK;
     void* ptrs[] = {c->blk_atom, c->blk_l, c->blk_ncon, c->blk_ao, c->blk_p0, c->blk_np, c->blk_exp, c->blk_coef,
                     c->sh_atom, c->sh_l, c->sh_ao, c->sh_p0, c->sh_np, c->sp_i, c->sp_j, c->sh_exp, c->sh_coef,
-                    c->charges, c->pa, c->pb, c->npp, c->slot, c->rec, c->Q, c->by_class, c->seg_begin,
-                    c->keys_in, c->sortedQ, c->sorted, c->counts_jk, c->counts_g, c->cub_tmp, c->boys, c->pos};
+                    c->charges, c->pa, c->pb, c->npp, c->slot, c->rec, c->Q, c->by_class, c->idx_in,
+                    c->tmp_idx, c->seg_id, c->seg_keys, c->seg_keys_out, c->seg_start, c->tmpQ, c->sortedQ,
+                    c->sorted, c->counts_jk, c->counts_g, c->cub_tmp, c->pos};
     for (void* p : ptrs) cudaFree(p);
+    for (int i = 0; i < NCLS; ++i) {
+        if (c->cls_stream[i]) cudaStreamDestroy(c->cls_stream[i]);
+        if (c->ev_join[i]) cudaEventDestroy(c->ev_join[i]);
+    }
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     delete c;
     return AIMD_OK;
 }
@@ -287,35 +285,71 @@ __global__ void pair_prep_kernel(int npair, const int* pa, const int* pb, const 
     npp[ip] = n;
 }
 
-__global__ void gather_keys_kernel(int n, const int* by_class, const double* Q, double* keys) {
+// Segment of each pair: angular class, primitive-pair bucket, contraction count.
+__global__ void segment_kernel(int npair, const int* pa, const int* pb, const int* blk_l, const int* blk_ncon,
+                               const int* npp, int* seg_id) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npair) return;
+    const int A = pa[p], B = pb[p];
+    const int nc = blk_ncon[A] * blk_ncon[B];
+    const int cb = nc >= 4 ? 2 : (nc >= 2 ? 1 : 0);
+    seg_id[p] = pcls(blk_l[A], blk_l[B]) * NSUB + npp_bucket(npp[p]) * NCONB + cb;
+}
+
+__global__ void gather_seg_kernel(int n, const int* order, const int* seg_id, int* keys) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) keys[i] = Q[by_class[i]];
+    if (i < n) keys[i] = seg_id[order[i]];
+}
+
+__global__ void gather_q_kernel(int n, const int* order, const double* Q, double* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = Q[order[i]];
+}
+
+// seg_start[y] = first sorted position with segment >= y (keys sorted ascending).
+__global__ void seg_start_kernel(int n, const int* keys, int* seg_start) {
+    const int y = blockIdx.x * blockDim.x + threadIdx.x;
+    if (y > NSEG) return;
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (keys[mid] < y) lo = mid + 1; else hi = mid;
+    }
+    seg_start[y] = lo;
 }
 
 struct ClsStart { int v[NCLS + 1]; };
 
-// counts[Y][s] = number of ket pairs of class Y (sorted prefix) kept with the
-// bra at sorted position s (class X >= Y), Q_s Q_j >= thr; cut at s for Y == X.
-__global__ void quartet_count_kernel(int npair, ClsStart cs, const double* sortedQ, double thr, int64_t* counts) {
+// counts[y][s] = number of ket pairs of segment y (a Q-sorted prefix) kept
+// with the bra at sorted position s (angular class X >= class of y),
+// Q_s Q_j >= thr; for y in class X only positions j <= s (each unordered
+// pair of pairs once).
+__global__ void quartet_count_kernel(int npair, ClsStart cs, const int* seg_start, const double* sortedQ, double thr,
+                                     int64_t* counts) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s > npair) return;
     if (s == npair) {
-        for (int y = 0; y < NCLS; ++y) counts[(size_t)y * (npair + 1) + npair] = 0;
+        for (int y = 0; y < NSEG; ++y) counts[(size_t)y * (npair + 1) + npair] = 0;
         return;
     }
     int X = 0;
     while (s >= cs.v[X + 1]) ++X;
     const double qs = sortedQ[s];
-    for (int y = 0; y < NCLS; ++y) {
+    for (int y = 0; y < NSEG; ++y) {
         int64_t cnt = 0;
-        if (y <= X) {
-            int lo = cs.v[y], hi = cs.v[y + 1];       // first j with qs*Q_j < thr
+        const int cy = y / NSUB;
+        if (cy <= X) {
+            const int y0 = seg_start[y], y1 = seg_start[y + 1];
+            int lo = y0, hi = y1;       // first j with qs*Q_j < thr
             while (lo < hi) {
                 const int mid = (lo + hi) >> 1;
                 if (qs * sortedQ[mid] >= thr) lo = mid + 1; else hi = mid;
             }
-            cnt = lo - cs.v[y];
-            if (y == X && cnt > s - cs.v[X] + 1) cnt = s - cs.v[X] + 1;
+            cnt = lo - y0;
+            if (cy == X) {
+                const int64_t cap = (int64_t)s + 1 - y0;
+                cnt = cap <= 0 ? 0 : (cnt > cap ? cap : cnt);
+            }
         }
         counts[(size_t)y * (npair + 1) + s] = cnt;
     }
@@ -328,10 +362,10 @@ QuartetArgs quartet_args(aimd_ctx* c, const int64_t* counts) {
     QuartetArgs q;
     q.pv = pair_view(c);
     q.bv = block_view(c);
-    q.boys = c->boys;
     q.sorted = c->sorted;
     q.sortedQ = c->sortedQ;
     q.counts = counts;
+    q.seg_start = c->seg_start;
     q.npair = c->npair;
     for (int i = 0; i <= NCLS; ++i) q.cls_start[i] = c->cls_start[i];
     q.nao = c->nao;
@@ -342,7 +376,7 @@ int build_counts(aimd_ctx* c, double thr, int64_t* counts, cudaStream_t st) {
     ClsStart cs;
     for (int i = 0; i <= NCLS; ++i) cs.v[i] = c->cls_start[i];
     const int n = c->npair + 1;
-    quartet_count_kernel<<<(n + 127) / 128, 128, 0, st>>>(c->npair, cs, c->sortedQ, thr, counts);
+    quartet_count_kernel<<<(n + 127) / 128, 128, 0, st>>>(c->npair, cs, c->seg_start, c->sortedQ, thr, counts);
     ++c->launches;
     CK(cudaGetLastError());
     return AIMD_OK;
@@ -362,6 +396,22 @@ LaunchEnv launch_env(aimd_ctx* c) {
     e.by_class = c->by_class;
     e.Q = c->Q;
     return e;
+}
+
+// all (CX, CY <= CX) gradient kernels of bra class CX, in order on one stream
+template <int CX>
+cudaError_t launch_grad_class(const LaunchEnv& e, const GradArgs& a, cudaStream_t st) {
+    cudaError_t r = cudaSuccess;
+#define AIMD_G1(X, Y) \
+    if (r == cudaSuccess && CX == X) r = launch_grad_c##X##_##Y(e, a, st);
+    AIMD_G1(0, 0)
+    AIMD_G1(1, 0) AIMD_G1(1, 1)
+    AIMD_G1(2, 0) AIMD_G1(2, 1) AIMD_G1(2, 2)
+    AIMD_G1(3, 0) AIMD_G1(3, 1) AIMD_G1(3, 2) AIMD_G1(3, 3)
+    AIMD_G1(4, 0) AIMD_G1(4, 1) AIMD_G1(4, 2) AIMD_G1(4, 3) AIMD_G1(4, 4)
+    AIMD_G1(5, 0) AIMD_G1(5, 1) AIMD_G1(5, 2) AIMD_G1(5, 3) AIMD_G1(5, 4) AIMD_G1(5, 5)
+#undef AIMD_G1
+    return r;
 }
 
 int class_status(aimd_ctx* c, cudaError_t r, const char* what, int cl) {
@@ -389,6 +439,32 @@ int class_status(aimd_ctx* c, cudaError_t r, const char* what, int cl) {
         if ((r_ = class_status(c, CALL(5), WHAT, 5))) return r_;            \
     } while (0)
 
+// The six class launches of one call run concurrently on the context's
+// class streams, forked from and joined back into the caller's stream, so
+// the long-running d-shell classes overlap the others.
+#define AIMD_EACH_CLASS_CONCURRENT(CALL, WHAT)                                        \
+    do {                                                                              \
+        CK(cudaEventRecord(c->ev_fork, st));                                          \
+        int r_ = AIMD_OK;                                                             \
+        for (int x_ = NCLS - 1; x_ >= 0 && r_ == AIMD_OK; --x_) {                     \
+            CK(cudaStreamWaitEvent(c->cls_stream[x_], c->ev_fork, 0));                \
+            cudaStream_t cs_ = c->cls_stream[x_];                                     \
+            cudaError_t e_ = cudaSuccess;                                             \
+            switch (x_) {                                                             \
+                case 0: e_ = CALL(0, cs_); break;                                     \
+                case 1: e_ = CALL(1, cs_); break;                                     \
+                case 2: e_ = CALL(2, cs_); break;                                     \
+                case 3: e_ = CALL(3, cs_); break;                                     \
+                case 4: e_ = CALL(4, cs_); break;                                     \
+                default: e_ = CALL(5, cs_); break;                                    \
+            }                                                                         \
+            r_ = class_status(c, e_, WHAT, x_);                                       \
+            CK(cudaEventRecord(c->ev_join[x_], cs_));                                 \
+            CK(cudaStreamWaitEvent(st, c->ev_join[x_], 0));                           \
+        }                                                                             \
+        if (r_) return r_;                                                            \
+    } while (0)
+
 }  // namespace
 
 extern "C" int aimd_set_geometry(aimd_ctx* c, const double* pos, void* stream) {
@@ -407,13 +483,20 @@ extern "C" int aimd_set_geometry(aimd_ctx* c, const double* pos, void* stream) {
         AIMD_EACH_CLASS(AIMD_SCHWARZ, "aimd_set_geometry/schwarz");
 #undef AIMD_SCHWARZ
     }
-    gather_keys_kernel<<<(np + 127) / 128, 128, 0, st>>>(np, c->by_class, c->Q, c->keys_in);
-    ++c->launches;
+    // order: Q descending, then (stable) by segment; segment starts on the device
+    const int nbk = (np + 127) / 128;
+    segment_kernel<<<nbk, 128, 0, st>>>(np, c->pa, c->pb, c->blk_l, c->blk_ncon, c->npp, c->seg_id);
     size_t bytes = c->cub_bytes;
-    CK(cub::DeviceSegmentedRadixSort::SortPairsDescending(c->cub_tmp, bytes, c->keys_in, c->sortedQ, c->by_class,
-                                                           c->sorted, np, NCLS, c->seg_begin, c->seg_begin + 1, 0,
-                                                           sizeof(double) * 8, st));
-    ++c->launches;
+    CK(cub::DeviceRadixSort::SortPairsDescending(c->cub_tmp, bytes, c->Q, c->tmpQ, c->idx_in, c->tmp_idx, np, 0,
+                                                 sizeof(double) * 8, st));
+    gather_seg_kernel<<<nbk, 128, 0, st>>>(np, c->tmp_idx, c->seg_id, c->seg_keys);
+    bytes = c->cub_bytes;
+    CK(cub::DeviceRadixSort::SortPairs(c->cub_tmp, bytes, c->seg_keys, c->seg_keys_out, c->tmp_idx, c->sorted, np, 0,
+                                       sizeof(int) * 8, st));
+    gather_q_kernel<<<nbk, 128, 0, st>>>(np, c->sorted, c->Q, c->sortedQ);
+    seg_start_kernel<<<1, NSEG + 1, 0, st>>>(np, c->seg_keys_out, c->seg_start);
+    c->launches += 6;
+    CK(cudaGetLastError());
     c->thr_jk = c->thr_g = -1.0;
     c->have_geometry = true;
     return AIMD_OK;
@@ -445,8 +528,8 @@ extern "C" int aimd_jk(aimd_ctx* c, int nset, const double* D, double* J, double
         a.D = D + s0 * nn;
         a.J = J + s0 * nn;
         a.K = K + s0 * nn;
-#define AIMD_JK(X) launch_jk_c##X(e, a, st)
-        AIMD_EACH_CLASS(AIMD_JK, "aimd_jk");
+#define AIMD_JK(X, S) launch_jk_c##X(e, a, S)
+        AIMD_EACH_CLASS_CONCURRENT(AIMD_JK, "aimd_jk");
 #undef AIMD_JK
     }
     return AIMD_OK;
@@ -522,8 +605,8 @@ extern "C" int aimd_grad2e(aimd_ctx* c, const double* Dc, int nx, const double* 
     a.grad = grad;
     a.natm = c->natm;
     const LaunchEnv e = launch_env(c);
-#define AIMD_GRAD(X) launch_grad_c##X(e, a, st)
-    AIMD_EACH_CLASS(AIMD_GRAD, "aimd_grad2e");
+#define AIMD_GRAD(X, S) launch_grad_class<X>(e, a, S)
+    AIMD_EACH_CLASS_CONCURRENT(AIMD_GRAD, "aimd_grad2e");
 #undef AIMD_GRAD
     return AIMD_OK;
 }
@@ -553,7 +636,7 @@ extern "C" int aimd_onee(aimd_ctx* c, const double* origin, double* S, double* T
                          void* stream) {
     if (!c || !S || !T || !M || !V || !c->have_geometry) return AIMD_ERR_ARG;
     int n = 0;
-    cudaError_t r = launch_onee(launch_env(c), shell_view(c), c->sp_cls_start, origin, c->boys, S, T, M, V,
+    cudaError_t r = launch_onee(launch_env(c), shell_view(c), c->sp_cls_start, origin, S, T, M, V,
                                 static_cast<cudaStream_t>(stream), &n);
     c->launches += n;
     CK(r);
@@ -563,7 +646,7 @@ extern "C" int aimd_onee(aimd_ctx* c, const double* origin, double* S, double* T
 extern "C" int aimd_onee_grad(aimd_ctx* c, const double* W, const double* D, double* grad, void* stream) {
     if (!c || !W || !D || !grad || !c->have_geometry) return AIMD_ERR_ARG;
     int n = 0;
-    cudaError_t r = launch_onee_grad(launch_env(c), shell_view(c), c->sp_cls_start, c->boys, W, D, grad,
+    cudaError_t r = launch_onee_grad(launch_env(c), shell_view(c), c->sp_cls_start, W, D, grad,
                                      static_cast<cudaStream_t>(stream), &n);
     c->launches += n;
     if (r == cudaErrorInvalidConfiguration) {
@@ -580,13 +663,14 @@ extern "C" int aimd_quartet_counts(aimd_ctx* c, int which, int64_t* out_host) {
     if (!c || !out_host || !c->have_geometry) return AIMD_ERR_ARG;
     const int64_t* counts = which ? c->counts_g : c->counts_jk;
     const int n = c->npair + 1;
-    std::vector<int64_t> h((size_t)NCLS * n);
+    std::vector<int64_t> h((size_t)NSEG * n);
     CK(cudaMemcpy(h.data(), counts, sizeof(int64_t) * h.size(), cudaMemcpyDeviceToHost));
     for (int x = 0; x < NCLS; ++x)
         for (int y = 0; y < NCLS; ++y) {
             int64_t t = 0;
             if (y <= x)
-                for (int s = c->cls_start[x]; s < c->cls_start[x + 1]; ++s) t += h[(size_t)y * n + s];
+                for (int sub = 0; sub < NSUB; ++sub)
+                    for (int s = c->cls_start[x]; s < c->cls_start[x + 1]; ++s) t += h[(size_t)(y * NSUB + sub) * n + s];
             out_host[x * NCLS + y] = t;
         }
     return AIMD_OK;

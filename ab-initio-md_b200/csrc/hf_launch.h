@@ -1,6 +1,8 @@
 // Host-side launchers of the class-templated kernels. Each bra pair class
-// lives in its own translation units (hf_class_jk.cu and hf_class_grad.cu
-// compiled with -DAIMD_CLASS=0..5) so that they compile in parallel.
+// lives in its own translation units (hf_class_jk.cu compiled with
+// -DAIMD_CLASS=0..5, hf_class_grad.cu with -DAIMD_CLASS=X -DAIMD_KET=Y for
+// Y <= X) so that they compile in parallel. Gradient launchers with Y > X
+// are declared but never defined or called.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -23,7 +25,12 @@ struct LaunchEnv {
 #define AIMD_DECLARE_CLASS(X)                                                                          \
     cudaError_t launch_schwarz_c##X(const LaunchEnv& e, const QuartetArgs& q, cudaStream_t st);         \
     cudaError_t launch_jk_c##X(const LaunchEnv& e, const JKArgs& a, cudaStream_t st);                    \
-    cudaError_t launch_grad_c##X(const LaunchEnv& e, const GradArgs& a, cudaStream_t st);
+    cudaError_t launch_grad_c##X##_0(const LaunchEnv& e, const GradArgs& a, cudaStream_t st);          \
+    cudaError_t launch_grad_c##X##_1(const LaunchEnv& e, const GradArgs& a, cudaStream_t st);          \
+    cudaError_t launch_grad_c##X##_2(const LaunchEnv& e, const GradArgs& a, cudaStream_t st);          \
+    cudaError_t launch_grad_c##X##_3(const LaunchEnv& e, const GradArgs& a, cudaStream_t st);          \
+    cudaError_t launch_grad_c##X##_4(const LaunchEnv& e, const GradArgs& a, cudaStream_t st);          \
+    cudaError_t launch_grad_c##X##_5(const LaunchEnv& e, const GradArgs& a, cudaStream_t st);
 AIMD_DECLARE_CLASS(0)
 AIMD_DECLARE_CLASS(1)
 AIMD_DECLARE_CLASS(2)
@@ -33,9 +40,9 @@ AIMD_DECLARE_CLASS(5)
 #undef AIMD_DECLARE_CLASS
 
 cudaError_t launch_onee(const LaunchEnv& e, const ShellView& sv, const int* sp_cls_start, const double* origin,
-                        const double* boys, double* S, double* T, double* M, double* V, cudaStream_t st, int* nlaunch);
-cudaError_t launch_onee_grad(const LaunchEnv& e, const ShellView& sv, const int* sp_cls_start, const double* boys,
-                             const double* W, const double* D, double* grad, cudaStream_t st, int* nlaunch);
+                        double* S, double* T, double* M, double* V, cudaStream_t st, int* nlaunch);
+cudaError_t launch_onee_grad(const LaunchEnv& e, const ShellView& sv, const int* sp_cls_start, const double* W,
+                             const double* D, double* grad, cudaStream_t st, int* nlaunch);
 
 inline cudaError_t set_smem_limit(const void* kernel, size_t bytes) {
     if (bytes > 227 * 1024) return cudaErrorInvalidConfiguration;

@@ -4,14 +4,14 @@
 namespace hf {
 
 cudaError_t launch_onee(const LaunchEnv& e, const ShellView& sv, const int* sp_cls_start, const double* origin,
-                        const double* boys, double* S, double* T, double* M, double* V, cudaStream_t st, int* nlaunch) {
+                        double* S, double* T, double* M, double* V, cudaStream_t st, int* nlaunch) {
     const double o[3] = {origin ? origin[0] : 0.0, origin ? origin[1] : 0.0, origin ? origin[2] : 0.0};
 #define AIMD_LAUNCH_1E(CL)                                                                                   \
     {                                                                                                        \
         const int b0 = sp_cls_start[CL], b1 = sp_cls_start[CL + 1];                                          \
         if (b1 > b0) {                                                                                       \
             onee_kernel<cls_la(CL), cls_lb(CL)><<<(b1 - b0 + 127) / 128, 128, 0, st>>>(sv, b0, b1, o[0], o[1], \
-                                                                                      o[2], boys, S, T, M, V); \
+                                                                                      o[2], S, T, M, V); \
             ++*nlaunch;                                                                                      \
         }                                                                                                    \
     }
@@ -20,15 +20,14 @@ cudaError_t launch_onee(const LaunchEnv& e, const ShellView& sv, const int* sp_c
     return cudaGetLastError();
 }
 
-cudaError_t launch_onee_grad(const LaunchEnv& e, const ShellView& sv, const int* sp_cls_start, const double* boys,
-                             const double* W, const double* D, double* grad, cudaStream_t st, int* nlaunch) {
+cudaError_t launch_onee_grad(const LaunchEnv& e, const ShellView& sv, const int* sp_cls_start, const double* W, const double* D, double* grad, cudaStream_t st, int* nlaunch) {
     const size_t smem = sizeof(double) * 3 * e.natm;
     if (smem > 48 * 1024) return cudaErrorInvalidConfiguration;
 #define AIMD_LAUNCH_1G(CL)                                                                                    \
     {                                                                                                         \
         const int b0 = sp_cls_start[CL], b1 = sp_cls_start[CL + 1];                                           \
         if (b1 > b0) {                                                                                        \
-            onee_grad_kernel<cls_la(CL), cls_lb(CL)><<<(b1 - b0 + 127) / 128, 128, smem, st>>>(sv, b0, b1, boys, W, \
+            onee_grad_kernel<cls_la(CL), cls_lb(CL)><<<(b1 - b0 + 127) / 128, 128, smem, st>>>(sv, b0, b1, W, \
                                                                                               D, grad);      \
             ++*nlaunch;                                                                                       \
         }                                                                                                     \

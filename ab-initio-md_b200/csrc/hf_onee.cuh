@@ -42,7 +42,7 @@ __device__ __forceinline__ double kin1d(const double (&e)[IM + 1][JM + 1][IM + J
 // pairs [p_begin, p_end) of the class-sorted shell-pair list.
 template <int LI, int LJ>
 __global__ void __launch_bounds__(128) onee_kernel(ShellView sv, int p_begin, int p_end, double ox, double oy,
-                                                   double oz, const double* boys, double* S, double* T,
+                                                   double oz, double* S, double* T,
                                                    double* M, double* V) {
     const int ip = p_begin + blockIdx.x * blockDim.x + threadIdx.x;
     if (ip >= p_end) return;
@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(128) onee_kernel(ShellView sv, int p_begin, in
             for (int c = 0; c < sv.natm; ++c) {
                 double R[nherm(L)];
                 hermite_r<L>(p, (Ax - sv.pos[3 * c]) - bp * ABx, (Ay - sv.pos[3 * c + 1]) - bp * ABy,
-                             (Az - sv.pos[3 * c + 2]) - bp * ABz, boys, R);
+                             (Az - sv.pos[3 * c + 2]) - bp * ABz, R);
                 const double w = -sv.charges[c] * 2.0 * PI / p;
 #pragma unroll
                 for (int h = 0; h < nherm(L); ++h) rsum[h] += w * R[h];
@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(128) onee_kernel(ShellView sv, int p_begin, in
 // d/dR [ sum W S + sum D T ] (W with the sign the caller wants) and
 // d/dR sum D V for shell pairs of class (LI, LJ); block-shared accumulator.
 template <int LI, int LJ>
-__global__ void __launch_bounds__(128) onee_grad_kernel(ShellView sv, int p_begin, int p_end, const double* boys,
+__global__ void __launch_bounds__(128) onee_grad_kernel(ShellView sv, int p_begin, int p_end,
                                                         const double* W, const double* Dm, double* grad) {
     extern __shared__ double gsh[];
     for (int i = threadIdx.x; i < 3 * sv.natm; i += blockDim.x) gsh[i] = 0.0;
@@ -238,7 +238,7 @@ __global__ void __launch_bounds__(128) onee_grad_kernel(ShellView sv, int p_begi
                 for (int c = 0; c < sv.natm; ++c) {
                     double R[NH1];
                     hermite_r<L + 1>(p, (Ax - sv.pos[3 * c]) - bp * ABx, (Ay - sv.pos[3 * c + 1]) - bp * ABy,
-                                     (Az - sv.pos[3 * c + 2]) - bp * ABz, boys, R);
+                                     (Az - sv.pos[3 * c + 2]) - bp * ABz, R);
                     const double pref = -sv.charges[c] * 2.0 * PI / p;
                     double ga[3] = {0.0, 0.0, 0.0}, gc[3] = {0.0, 0.0, 0.0};
 #pragma unroll
