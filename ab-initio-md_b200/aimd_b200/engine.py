@@ -151,6 +151,16 @@ class Engine:
                                     _stream()), "aimd_jk")
         return J, K
 
+    def jk_delta_acc(self, dD: torch.Tensor, thr: float, dthr: float) -> tuple[torch.Tensor, torch.Tensor]:
+        """Accumulators of J/K for difference densities with density-weighted screening."""
+        dD = dD.contiguous()
+        J = torch.empty_like(dD)
+        K = torch.empty_like(dD)
+        _lib.check(self.lib.aimd_jk_delta(self.handle, dD.shape[0], ctypes.c_void_p(dD.data_ptr()),
+                                          ctypes.c_void_p(J.data_ptr()), ctypes.c_void_p(K.data_ptr()), float(thr),
+                                          float(dthr), _stream()), "aimd_jk_delta")
+        return J, K
+
     def eri_tensor(self, thr: float) -> torch.Tensor:
         n = self.nao
         eri = torch.empty((n, n, n, n), dtype=torch.float64, device=self.device)

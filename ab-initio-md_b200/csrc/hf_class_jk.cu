@@ -28,7 +28,7 @@ cudaError_t AIMD_CAT(launch_jk_c, AIMD_CLASS)(const LaunchEnv& e, const JKArgs& 
     const size_t smem = jk_smem_bytes<CX, 1>(e.nao, e.maxbp[CX]);
     cudaError_t r = set_smem_limit((const void*)jk_bra_kernel<CX, 1>, smem);
     if (r != cudaSuccess) return r;
-    jk_bra_kernel<CX, 1><<<cnt, 128, smem, st>>>(a);
+    jk_bra_kernel<CX, 1><<<cnt * JKKernel<CX, 1>::NY, JK_THREADS, smem, st>>>(a);
     return cudaGetLastError();
 }
 

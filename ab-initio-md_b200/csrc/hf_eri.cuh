@@ -31,8 +31,8 @@ struct QClass {
     static constexpr int KAB = KA * KB, KCD = KC * KD;
     static constexpr int NROW = KAB * NAB;
     // ket contraction combinations per thread item: all of them unless the
-    // per-thread accumulator v[NROW][KG] would exceed 48 doubles
-    static constexpr int KG = NROW * KCD <= 48 ? KCD : ((KCD % 2 == 0 && NROW * 2 <= 48) ? 2 : 1);
+    // per-thread accumulator v[NROW][KG] would exceed 24 doubles
+    static constexpr int KG = NROW * KCD <= 24 ? KCD : ((KCD % 2 == 0 && NROW * 2 <= 24) ? 2 : 1);
     static constexpr int NKG = KCD / KG;
     static constexpr int NHB = nherm(LAB);
 };
@@ -265,6 +265,11 @@ struct JKArgs {
     const double* D;    // [nset][nao][nao], symmetric
     double* J;          // un-symmetrised accumulators, same shape
     double* K;
+    // density-weighted screening (difference densities): skip a quartet when
+    // Q1 Q2 max|D| over its six density blocks < dthr; bmax = nullptr: off
+    const double* bmax; // [nblock][nblock] max |D| per block pair (all sets)
+    int nblock;
+    double dthr;
 };
 
 // Digest one column (fixed ket component pair cd, all ket contractions kk)
@@ -276,7 +281,7 @@ struct JKArgs {
 // (m in A, n in B, l in C, s in D); the host forms J + J^T and K + K^T.
 // K rows m, n belong to the bra pair: Ksm[set][slot][col], slot < KA*NA for
 // A's functions, then B's.
-template <int CX, int CY, int NS>
+template <int CX, int CY, int NS, bool KGLOBAL>
 __device__ __forceinline__ void jk_digest_column(const JKArgs& a, const BraStage& st, int P2, int C, int Dd, int ic,
                                                  int id, int kg,
                                                  const double (&v)[QClass<CX, CY>::NROW][QClass<CX, CY>::KG],
@@ -292,7 +297,10 @@ __device__ __forceinline__ void jk_digest_column(const JKArgs& a, const BraStage
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
         const double* __restrict__ D = a.D + s * nn;
-        double* Ks = Ksm + (size_t)s * NF * n;
+        // K rows of the bra functions: shared accumulator, or the global K
+        // itself (KGLOBAL, for bra classes whose rows would not fit)
+        double* Ks = KGLOBAL ? nullptr : Ksm + (size_t)s * NF * n;
+        double* Kg = a.K + s * nn;
 #pragma unroll
         for (int kk = 0; kk < Q::KG; ++kk) {
                 const int kq = kg * Q::KG + kk, kc = kq / Q::KD, kd = kq % Q::KD;
@@ -333,7 +341,8 @@ __device__ __forceinline__ void jk_digest_column(const JKArgs& a, const BraStage
                                 s1 += v[r][kk] * __ldg(D + nb_ * n + sg);
                                 s2 += v[r][kk] * __ldg(D + nb_ * n + l);
                             }
-                        double* row = Ks + (size_t)(ka * Q::NA + ia) * n;
+                        double* row = KGLOBAL ? Kg + (size_t)(st.oA + ka * Q::NA + ia) * n
+                                              : Ks + (size_t)(ka * Q::NA + ia) * n;
                         atomicAdd(row + l, g * s1);
                         atomicAdd(row + sg, g * s2);
                     }
@@ -354,7 +363,8 @@ __device__ __forceinline__ void jk_digest_column(const JKArgs& a, const BraStage
                                 s1 += v[r][kk] * __ldg(D + m * n + sg);
                                 s2 += v[r][kk] * __ldg(D + m * n + l);
                             }
-                        double* row = Ks + (size_t)(NFA + kb * Q::NB + jb) * n;
+                        double* row = KGLOBAL ? Kg + (size_t)(st.oB + kb * Q::NB + jb) * n
+                                              : Ks + (size_t)(NFA + kb * Q::NB + jb) * n;
                         atomicAdd(row + l, g * s1);
                         atomicAdd(row + sg, g * s2);
                     }
@@ -363,7 +373,7 @@ __device__ __forceinline__ void jk_digest_column(const JKArgs& a, const BraStage
 }
 
 // Items of ket class CY for the staged bra pair.
-template <int CX, int CY, int NS>
+template <int CX, int CY, int NS, bool KGLOBAL>
 __device__ __forceinline__ void jk_ket_class(const JKArgs& a, const BraStage& st, int spos, double* Jt, double* Ksm) {
     using Q = QClass<CX, CY>;
     for (int sub = 0; sub < NSUB; ++sub) {
@@ -377,10 +387,17 @@ __device__ __forceinline__ void jk_ket_class(const JKArgs& a, const BraStage& st
             const int jj = static_cast<int>(it / (Q::NCD * Q::NKG)), cd = static_cast<int>((it / Q::NKG) % Q::NCD);
             const int P2 = a.q.sorted[j0 + jj];
             const int C = a.q.pv.pa_blk[P2], Dd = a.q.pv.pb_blk[P2];
+            if (a.bmax) {
+                const double* bm = a.bmax;
+                const int nb = a.nblock;
+                double dm = fmax(fmax(bm[st.A * nb + st.B], bm[C * nb + Dd]),
+                                 fmax(fmax(bm[st.A * nb + C], bm[st.A * nb + Dd]), fmax(bm[st.B * nb + C], bm[st.B * nb + Dd])));
+                if (a.q.sortedQ[spos] * a.q.sortedQ[j0 + jj] * dm < a.dthr) continue;
+            }
             const int ic = cd / Q::ND, id = cd % Q::ND;
             double v[Q::NROW][Q::KG];
             eri_column<CX, CY>(st, a.q.pv.rec + a.q.pv.slot[P2] * PPW, a.q.pv.npp[P2], ic, id, kg, v);
-            jk_digest_column<CX, CY, NS>(a, st, P2, C, Dd, ic, id, kg, v, Jt, Ksm);
+            jk_digest_column<CX, CY, NS, KGLOBAL>(a, st, P2, C, Dd, ic, id, kg, v, Jt, Ksm);
         }
     }
 }
@@ -391,10 +408,16 @@ struct JKKernel {
     static constexpr int NROW = Q0::NROW;
     static constexpr int NF = Q0::KA * Q0::NA + Q0::KB * Q0::NB;
     static constexpr int ESIZE = BraE<Q0::LA, Q0::LB, 0>::SIZE;
+    // d-bra classes: one CTA per (bra pair, ket class), shorter CTAs that
+    // fill the machine; dd bras accumulate K in global memory
+    static constexpr bool SPLIT = CX >= 3;
+    static constexpr int NY = SPLIT ? CX + 1 : 1;
+    static constexpr bool KGLOBAL = CX == 5;
+    static constexpr int KROWS = KGLOBAL ? 0 : NS * NF;
 };
 
-// Dynamic shared memory: K rows [NS][NF][nao], per-thread J_ab slots
-// [NS][NROW][blockDim], bra E tables.
+// Dynamic shared memory: K rows [NS][NF][nao] (unless KGLOBAL), per-thread
+// J_ab slots [NS][NROW][blockDim], bra stage.
 constexpr int JK_THREADS = 128;
 
 template <int CX, int NS>
@@ -404,22 +427,33 @@ __global__ void __launch_bounds__(JK_THREADS) jk_bra_kernel(JKArgs a) {
     extern __shared__ double smem[];
     const int n = a.q.nao;
     double* Ksm = smem;
-    double* Jt = Ksm + (size_t)NS * KK::NF * n;
+    double* Jt = Ksm + (size_t)KK::KROWS * n;
     double* Esm = Jt + NS * KK::NROW * JK_THREADS;
-    const int spos = a.q.cls_start[CX] + blockIdx.x;
+    const int yk = KK::SPLIT ? (int)(blockIdx.x % KK::NY) : -1;
+    const int spos = a.q.cls_start[CX] + (int)(blockIdx.x / KK::NY);
     const int P1 = a.q.sorted[spos];
     __shared__ BraStage st;
-    if (threadIdx.x == 0) load_stage(a.q, P1, st, Esm);
-    for (int i = threadIdx.x; i < NS * KK::NF * n + NS * KK::NROW * JK_THREADS; i += blockDim.x) smem[i] = 0.0;
+    __shared__ int any;
+    if (threadIdx.x == 0) {
+        load_stage(a.q, P1, st, Esm);
+        int64_t tot = 0;
+        for (int y = 0; y <= CX; ++y)
+            if (yk < 0 || y == yk)
+                for (int sub = 0; sub < NSUB; ++sub) tot += a.q.counts[(size_t)(y * NSUB + sub) * (a.q.npair + 1) + spos];
+        any = tot > 0;
+    }
     __syncthreads();
+    if (!any) return;
+    for (int i = threadIdx.x; i < KK::KROWS * n + NS * KK::NROW * JK_THREADS; i += blockDim.x) smem[i] = 0.0;
     stage_bra_e<Q0::LA, Q0::LB, 0>(st);
     __syncthreads();
-    jk_ket_class<CX, 0, NS>(a, st, spos, Jt, Ksm);
-    if constexpr (CX >= 1) jk_ket_class<CX, 1, NS>(a, st, spos, Jt, Ksm);
-    if constexpr (CX >= 2) jk_ket_class<CX, 2, NS>(a, st, spos, Jt, Ksm);
-    if constexpr (CX >= 3) jk_ket_class<CX, 3, NS>(a, st, spos, Jt, Ksm);
-    if constexpr (CX >= 4) jk_ket_class<CX, 4, NS>(a, st, spos, Jt, Ksm);
-    if constexpr (CX >= 5) jk_ket_class<CX, 5, NS>(a, st, spos, Jt, Ksm);
+    constexpr bool KG_ = KK::KGLOBAL;
+    if (yk < 0 || yk == 0) jk_ket_class<CX, 0, NS, KG_>(a, st, spos, Jt, Ksm);
+    if constexpr (CX >= 1) if (yk < 0 || yk == 1) jk_ket_class<CX, 1, NS, KG_>(a, st, spos, Jt, Ksm);
+    if constexpr (CX >= 2) if (yk < 0 || yk == 2) jk_ket_class<CX, 2, NS, KG_>(a, st, spos, Jt, Ksm);
+    if constexpr (CX >= 3) if (yk < 0 || yk == 3) jk_ket_class<CX, 3, NS, KG_>(a, st, spos, Jt, Ksm);
+    if constexpr (CX >= 4) if (yk < 0 || yk == 4) jk_ket_class<CX, 4, NS, KG_>(a, st, spos, Jt, Ksm);
+    if constexpr (CX >= 5) if (yk < 0 || yk == 5) jk_ket_class<CX, 5, NS, KG_>(a, st, spos, Jt, Ksm);
     __syncthreads();
     const size_t nn = (size_t)n * n;
     // flush J_ab: one thread per (set, row) sums the per-thread slots
@@ -434,20 +468,22 @@ __global__ void __launch_bounds__(JK_THREADS) jk_bra_kernel(JKArgs a) {
         atomicAdd(a.J + s * nn + (size_t)m * n + nb_, val);
     }
     // flush K rows
-    constexpr int NFA = Q0::KA * Q0::NA;
-    for (int i = threadIdx.x; i < NS * KK::NF * n; i += blockDim.x) {
-        const double val = Ksm[i];
-        if (val == 0.0) continue;
-        const int col = i % n, f = (i / n) % KK::NF, s = i / (n * KK::NF);
-        const int row = f < NFA ? st.oA + f : st.oB + (f - NFA);
-        atomicAdd(a.K + s * nn + (size_t)row * n + col, val);
+    if constexpr (!KK::KGLOBAL) {
+        constexpr int NFA = Q0::KA * Q0::NA;
+        for (int i = threadIdx.x; i < KK::KROWS * n; i += blockDim.x) {
+            const double val = Ksm[i];
+            if (val == 0.0) continue;
+            const int col = i % n, f = (i / n) % KK::NF, s = i / (n * KK::NF);
+            const int row = f < NFA ? st.oA + f : st.oB + (f - NFA);
+            atomicAdd(a.K + s * nn + (size_t)row * n + col, val);
+        }
     }
 }
 
 template <int CX, int NS>
 size_t jk_smem_bytes(int nao, int max_bra_prims) {
     using KK = JKKernel<CX, NS>;
-    return sizeof(double) * ((size_t)NS * KK::NF * nao + (size_t)NS * KK::NROW * JK_THREADS +
+    return sizeof(double) * ((size_t)KK::KROWS * nao + (size_t)NS * KK::NROW * JK_THREADS +
                              (size_t)max_bra_prims * (KK::ESIZE + SBW));
 }
 

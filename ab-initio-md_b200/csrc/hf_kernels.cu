@@ -66,6 +66,9 @@ struct aimd_ctx {
     int* sorted;
     int64_t* counts_jk;     // [NSEG][npair + 1] kept ket prefix per (ket segment, bra position)
     int64_t* counts_g;
+    int64_t* counts_d;      // difference-density builds (threshold changes every call)
+    double* bmax;           // [nblock][nblock] max |D| per block pair
+    double* dmax;           // [1] max over bmax
     cudaStream_t cls_stream[NCLS];
     cudaEvent_t ev_fork, ev_join[NCLS];
     int maxbp[NCLS];        // largest primitive-pair count of a block pair, per class
@@ -203,6 +206,9 @@ extern "C" int aimd_create(aimd_ctx** out, int natm, int nao, int nblock, const 
         CK(dalloc(&c->sorted, np));
         CK(dalloc(&c->counts_jk, (size_t)NSEG * (np + 1)));
         CK(dalloc(&c->counts_g, (size_t)NSEG * (np + 1)));
+        CK(dalloc(&c->counts_d, (size_t)NSEG * (np + 1)));
+        CK(dalloc(&c->bmax, (size_t)nblock * nblock));
+        CK(dalloc(&c->dmax, 1));
         for (int cl = 0; cl < NCLS; ++cl) c->maxbp[cl] = 1;
         for (int p = 0; p < np; ++p)
             c->maxbp[cls[p]] = std::max(c->maxbp[cls[p]], blk_np[pa[p]] * blk_np[pb[p]]);
@@ -227,7 +233,7 @@ extern "C" int aimd_destroy(aimd_ctx* c) {
                     c->sh_atom, c->sh_l, c->sh_ao, c->sh_p0, c->sh_np, c->sp_i, c->sp_j, c->sh_exp, c->sh_coef,
                     c->charges, c->pa, c->pb, c->npp, c->slot, c->rec, c->Q, c->by_class, c->idx_in,
                     c->tmp_idx, c->seg_id, c->seg_keys, c->seg_keys_out, c->seg_start, c->tmpQ, c->sortedQ,
-                    c->sorted, c->counts_jk, c->counts_g, c->cub_tmp, c->pos};
+                    c->sorted, c->counts_jk, c->counts_g, c->counts_d, c->bmax, c->dmax, c->cub_tmp, c->pos};
     for (void* p : ptrs) cudaFree(p);
     for (int i = 0; i < NCLS; ++i) {
         if (c->cls_stream[i]) cudaStreamDestroy(c->cls_stream[i]);
@@ -325,8 +331,10 @@ struct ClsStart { int v[NCLS + 1]; };
 // Q_s Q_j >= thr; for y in class X only positions j <= s (each unordered
 // pair of pairs once).
 __global__ void quartet_count_kernel(int npair, ClsStart cs, const int* seg_start, const double* sortedQ, double thr,
-                                     int64_t* counts) {
+                                     const double* thr_div, double thr_floor, int64_t* counts) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    // density-weighted enumeration: max(floor, thr / max|D|)
+    if (thr_div) thr = *thr_div > 0.0 ? fmax(thr_floor, thr / *thr_div) : INFINITY;
     if (s > npair) return;
     if (s == npair) {
         for (int y = 0; y < NSEG; ++y) counts[(size_t)y * (npair + 1) + npair] = 0;
@@ -355,6 +363,34 @@ __global__ void quartet_count_kernel(int npair, ClsStart cs, const int* seg_star
     }
 }
 
+// bmax[I][J] = max over the functions of blocks I, J and the sets of |D|
+__global__ void block_dmax_kernel(int nblock, int nao, int nset, const int* blk_l, const int* blk_ncon,
+                                  const int* blk_ao, const double* D, double* bmax) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nblock * nblock) return;
+    const int I = i / nblock, J = i % nblock;
+    const int nI = blk_ncon[I] * ncart(blk_l[I]), nJ = blk_ncon[J] * ncart(blk_l[J]);
+    const size_t nn = (size_t)nao * nao;
+    double m = 0.0;
+    for (int s = 0; s < nset; ++s)
+        for (int a = 0; a < nI; ++a)
+            for (int b = 0; b < nJ; ++b) m = fmax(m, fabs(D[s * nn + (size_t)(blk_ao[I] + a) * nao + blk_ao[J] + b]));
+    bmax[i] = m;
+}
+
+__global__ void max_reduce_kernel(int n, const double* x, double* out) {
+    __shared__ double sm[256];
+    double m = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, x[i]);
+    sm[threadIdx.x] = m;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = sm[0];
+}
+
 PairView pair_view(aimd_ctx* c) { return PairView{c->pa, c->pb, c->slot, c->npp, c->rec}; }
 BlockView block_view(aimd_ctx* c) { return BlockView{c->blk_atom, c->blk_l, c->blk_ncon, c->blk_ao}; }
 
@@ -372,11 +408,13 @@ QuartetArgs quartet_args(aimd_ctx* c, const int64_t* counts) {
     return q;
 }
 
-int build_counts(aimd_ctx* c, double thr, int64_t* counts, cudaStream_t st) {
+int build_counts(aimd_ctx* c, double thr, int64_t* counts, cudaStream_t st, const double* thr_div = nullptr,
+                 double thr_floor = 0.0) {
     ClsStart cs;
     for (int i = 0; i <= NCLS; ++i) cs.v[i] = c->cls_start[i];
     const int n = c->npair + 1;
-    quartet_count_kernel<<<(n + 127) / 128, 128, 0, st>>>(c->npair, cs, c->seg_start, c->sortedQ, thr, counts);
+    quartet_count_kernel<<<(n + 127) / 128, 128, 0, st>>>(c->npair, cs, c->seg_start, c->sortedQ, thr, thr_div,
+                                                           thr_floor, counts);
     ++c->launches;
     CK(cudaGetLastError());
     return AIMD_OK;
@@ -528,6 +566,9 @@ extern "C" int aimd_jk(aimd_ctx* c, int nset, const double* D, double* J, double
         a.D = D + s0 * nn;
         a.J = J + s0 * nn;
         a.K = K + s0 * nn;
+        a.bmax = nullptr;
+        a.nblock = c->nblock;
+        a.dthr = 0.0;
 #define AIMD_JK(X, S) launch_jk_c##X(e, a, S)
         AIMD_EACH_CLASS_CONCURRENT(AIMD_JK, "aimd_jk");
 #undef AIMD_JK
@@ -553,6 +594,42 @@ __global__ void scatter_slice_kernel(int n, int l, int s, const double* J, doubl
     eri[((m * N + nn_) * N + s) * N + l] = v;
 }
 }  // namespace
+
+// J/K accumulators of a change of density (incremental Fock builds): a
+// quartet is skipped when Q_ab Q_cd max|dD| < dthr, max over the six block
+// pairs of dD that it touches (density-weighted Schwarz screening).
+extern "C" int aimd_jk_delta(aimd_ctx* c, int nset, const double* D, double* J, double* K, double thr, double dthr,
+                             void* stream) {
+    if (!c || !D || !J || !K || nset < 1 || !c->have_geometry || !(dthr > 0.0)) return AIMD_ERR_ARG;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t nn = (size_t)c->nao * c->nao;
+    const int nb2 = c->nblock * c->nblock;
+    block_dmax_kernel<<<(nb2 + 127) / 128, 128, 0, st>>>(c->nblock, c->nao, nset, c->blk_l, c->blk_ncon, c->blk_ao, D,
+                                                         c->bmax);
+    max_reduce_kernel<<<1, 256, 0, st>>>(nb2, c->bmax, c->dmax);
+    c->launches += 2;
+    CK(cudaGetLastError());
+    // enumerate at max(thr, dthr / max|D|): the integral screen still holds,
+    // and no quartet that the density-weighted test keeps is missed
+    if (int r = build_counts(c, dthr, c->counts_d, st, c->dmax, thr)) return r;
+    CK(cudaMemsetAsync(J, 0, sizeof(double) * nset * nn, st));
+    CK(cudaMemsetAsync(K, 0, sizeof(double) * nset * nn, st));
+    const LaunchEnv e = launch_env(c);
+    for (int s0 = 0; s0 < nset; ++s0) {
+        JKArgs a;
+        a.q = quartet_args(c, c->counts_d);
+        a.D = D + s0 * nn;
+        a.J = J + s0 * nn;
+        a.K = K + s0 * nn;
+        a.bmax = c->bmax;
+        a.nblock = c->nblock;
+        a.dthr = dthr;
+#define AIMD_JK(X, S) launch_jk_c##X(e, a, S)
+        AIMD_EACH_CLASS_CONCURRENT(AIMD_JK, "aimd_jk_delta");
+#undef AIMD_JK
+    }
+    return AIMD_OK;
+}
 
 // Test and debug sizes only: the tensor is probed column by column through
 // the integral-direct Coulomb build (J[D] with D the symmetric unit matrix

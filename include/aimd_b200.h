@@ -61,6 +61,15 @@ int aimd_pair_count(aimd_ctx *ctx);
  * Replaces eri_tensor + jk_from_eri (aimd/qc/integrals.py:986-1044). */
 int aimd_jk(aimd_ctx *ctx, int nset, const double *D, double *J, double *K, double thr, void *stream);
 
+/* J/K of difference densities D[nset][nao][nao] (device), for incremental
+ * Fock builds: quartets with Q1 Q2 < thr are skipped as in aimd_jk, and so
+ * are quartets with Q1 Q2 max|D| < dthr, max over the six density blocks
+ * the quartet touches (density-weighted Schwarz screening). Same output
+ * convention as aimd_jk. No counterpart in the reference, which rebuilds
+ * J/K from the full density every iteration (aimd/qc/scf.py:863-867). */
+int aimd_jk_delta(aimd_ctx *ctx, int nset, const double *D, double *J, double *K, double thr, double dthr,
+                  void *stream);
+
 /* Full screened tensor eri[nao^4] (device), test/debug sizes only.
  * aimd/qc/integrals.py:986-1006 (eri_tensor). */
 int aimd_eri_tensor(aimd_ctx *ctx, double *eri, double thr, void *stream);

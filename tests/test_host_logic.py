@@ -52,6 +52,9 @@ def test_scf_options_and_electron_counts():
         SCFOptions(conv_energy=0.0)
     with pytest.raises(ValueError):
         SCFOptions(damping=1.0)
+    with pytest.raises(ValueError):
+        SCFOptions(fock_rebuild=0)
+    assert SCFOptions().incremental_fock and SCFOptions(incremental_fock=False).fock_rebuild >= 1
     assert electron_counts(10, 0, 1, "rhf") == (5, 5)
     assert electron_counts(9, 0, 2) == (5, 4)
     with pytest.raises(ValueError):
