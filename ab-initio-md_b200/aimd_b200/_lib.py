@@ -34,6 +34,7 @@ SIGNATURES = {
     "aimd_jk": (_i, [_vp, _i, _vp, _vp, _vp, _d, _vp]),
     "aimd_jk_delta": (_i, [_vp, _i, _vp, _vp, _vp, _d, _d, _vp]),
     "aimd_eri_tensor": (_i, [_vp, _vp, _d, _vp]),
+    "aimd_eri_tensor_static": (_i, [_vp, _vp, _d, _vp]),
     "aimd_grad2e": (_i, [_vp, _vp, _i, _vp, _d, _d, _d, _vp, _vp]),
     "aimd_onee": (_i, [_vp, _f64p, _vp, _vp, _vp, _vp, _vp]),
     "aimd_onee_grad": (_i, [_vp, _vp, _vp, _vp, _vp]),

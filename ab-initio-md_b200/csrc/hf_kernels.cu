@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "../../include/aimd_b200.h"
@@ -658,6 +659,81 @@ extern "C" int aimd_eri_tensor(aimd_ctx* c, double* eri, double thr, void* strea
     cudaFree(scratch);
     if (status != AIMD_OK) return status;
     CK(e1);
+    return AIMD_OK;
+}
+
+// Scratch of aimd_eri_tensor_static: D, J and K of one probe for up to
+// AIMD_ERI_STATIC_MAX_NAO AOs (3 x 128^2 doubles = 384 KiB per device),
+// in the module's static device memory instead of cudaMalloc.
+static __device__ __align__(256) double g_eri_static_scratch[3 * AIMD_ERI_STATIC_MAX_NAO * AIMD_ERI_STATIC_MAX_NAO];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_eri_static_mu;
+double* g_eri_static_ptr[kMaxDevices] = {};
+
+// Device address of the scratch on the current device, looked up once per
+// device (the first call on each device does this set-up).
+int eri_static_scratch(double** out) {
+    int dev = -1;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) {
+        snprintf(g_err, sizeof g_err, "aimd_eri_tensor_static: device ordinal %d beyond %d", dev, kMaxDevices);
+        return AIMD_ERR_UNSUPPORTED;
+    }
+    std::lock_guard<std::mutex> lock(g_eri_static_mu);
+    if (!g_eri_static_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_eri_static_scratch);
+        if (e != cudaSuccess || !p) {
+            snprintf(g_err, sizeof g_err, "aimd_eri_tensor_static: cudaGetSymbolAddress: %s",
+                     cudaGetErrorString(e));
+            return AIMD_ERR_CUDA;
+        }
+        g_eri_static_ptr[dev] = static_cast<double*>(p);
+    }
+    *out = g_eri_static_ptr[dev];
+    return AIMD_OK;
+}
+}  // namespace
+
+// aimd_eri_tensor without any allocation: the D/J/K probe scratch is the
+// static array above, so nao <= AIMD_ERI_STATIC_MAX_NAO. Nothing in the
+// scratch has to start at zero (each probe writes all of D, and aimd_jk
+// clears J and K); every element of eri is written. Asynchronous on stream.
+extern "C" int aimd_eri_tensor_static(aimd_ctx* c, double* eri, double thr, void* stream) {
+    if (!c || !eri || !c->have_geometry) return AIMD_ERR_ARG;
+    const int n = c->nao;
+    if (n > AIMD_ERI_STATIC_MAX_NAO) {
+        snprintf(g_err, sizeof g_err, "aimd_eri_tensor_static: %d AOs exceed the static scratch limit of %d AOs "
+                 "(use aimd_eri_tensor)", n, AIMD_ERI_STATIC_MAX_NAO);
+        return AIMD_ERR_ARG;
+    }
+    // the context's buffers must live on the current device, like the scratch
+    cudaPointerAttributes pa;
+    CK(cudaPointerGetAttributes(&pa, c->rec));
+    int dev = -1;
+    CK(cudaGetDevice(&dev));
+    if (pa.device != dev) {
+        snprintf(g_err, sizeof g_err, "aimd_eri_tensor_static: context on device %d, current device %d",
+                 pa.device, dev);
+        return AIMD_ERR_ARG;
+    }
+    double* scratch = nullptr;
+    if (int r = eri_static_scratch(&scratch)) return r;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t nn = (size_t)n * n;
+    double *D = scratch, *J = scratch + nn, *K = scratch + 2 * nn;
+    const int blocks = (int)((nn + 255) / 256);
+    for (int l = 0; l < n; ++l)
+        for (int s = 0; s <= l; ++s) {
+            unit_density_kernel<<<blocks, 256, 0, st>>>(n, l, s, D);
+            ++c->launches;
+            if (int r = aimd_jk(c, 1, D, J, K, thr, stream)) return r;
+            scatter_slice_kernel<<<blocks, 256, 0, st>>>(n, l, s, J, eri);
+            ++c->launches;
+        }
+    CK(cudaGetLastError());
     return AIMD_OK;
 }
 

@@ -74,6 +74,22 @@ int aimd_jk_delta(aimd_ctx *ctx, int nset, const double *D, double *J, double *K
  * aimd/qc/integrals.py:986-1006 (eri_tensor). */
 int aimd_eri_tensor(aimd_ctx *ctx, double *eri, double thr, void *stream);
 
+/* aimd_eri_tensor for callers that may not allocate device memory: the same
+ * tensor with the probe scratch (D, J, K of one unit-density Coulomb build)
+ * in a static device array of the library instead of cudaMalloc/cudaFree.
+ * No counterpart in the reference.
+ *   - nao <= AIMD_ERI_STATIC_MAX_NAO (128, 384 KiB of scratch per device);
+ *     larger sizes return AIMD_ERR_ARG with a message, before any work;
+ *   - the context's device must be current; the first call on each device
+ *     looks up the scratch address (cudaGetSymbolAddress) and should come
+ *     before any stream capture;
+ *   - nothing has to be zeroed by the caller; asynchronous on stream (the
+ *     tensor is ready when the stream is), unlike aimd_eri_tensor;
+ *   - the scratch is one per device: calls that overlap on one device (other
+ *     streams, threads or contexts) race and must be serialised by the caller. */
+#define AIMD_ERI_STATIC_MAX_NAO 128
+int aimd_eri_tensor_static(aimd_ctx *ctx, double *eri, double thr, void *stream);
+
 /* d/dR of 1/2 sum Gamma (mn|ls), Gamma from Dc [nao][nao] and Dx
  * [nx][nao][nao] with exchange factor kfac; grad [natm][3] (device).
  * gamma_bound >= max|Gamma| over all quartets (enumeration bound); the exact
