@@ -373,32 +373,76 @@ __device__ __forceinline__ void jk_digest_column(const JKArgs& a, const BraStage
 }
 
 // Items of ket class CY for the staged bra pair.
+// Work queue of one CTA: the ket pairs of a segment that pass a per-pair
+// test are compacted into shared memory in chunks of KQ_CAP (warp ballots,
+// one shared atomic per warp), then dealt to the threads as NPER items each,
+// so that lanes only receive live work. Dealing starts where the previous
+// chunk ended (rot), so ragged tails do not pile up on the low threads.
+// Every thread of the CTA must call this with the same j0 and cnt.
+constexpr int KQ_CAP = 256;
+struct KetQueue {
+    int pos[KQ_CAP];
+    int n;
+};
+
+template <int NPER, typename Keep, typename Work>
+__device__ __forceinline__ void ket_items(int j0, int64_t cnt, KetQueue& q, int& rot, Keep keep, Work work) {
+    const int lane = threadIdx.x & 31;
+    for (int64_t base = 0; base < cnt; base += KQ_CAP) {
+        const int m = static_cast<int>(cnt - base < KQ_CAP ? cnt - base : KQ_CAP);
+        if (threadIdx.x == 0) q.n = 0;
+        __syncthreads();
+        for (int i0 = 0; i0 < m; i0 += blockDim.x) {
+            const int i = i0 + threadIdx.x;
+            const int pos = j0 + static_cast<int>(base) + i;
+            const bool k = i < m && keep(pos);
+            const unsigned mask = __ballot_sync(0xffffffffu, k);
+            int w0 = 0;
+            if (lane == 0 && mask) w0 = atomicAdd(&q.n, __popc(mask));
+            w0 = __shfl_sync(0xffffffffu, w0, 0);
+            if (k) q.pos[w0 + __popc(mask & ((1u << lane) - 1u))] = pos;
+        }
+        __syncthreads();
+        const int items = q.n * NPER;
+        int it = static_cast<int>(threadIdx.x) - rot;
+        if (it < 0) it += blockDim.x;
+        for (; it < items; it += blockDim.x) work(q.pos[it / NPER], it % NPER);
+        rot = (rot + items) % static_cast<int>(blockDim.x);
+        __syncthreads();
+    }
+}
+
 template <int CX, int CY, int NS, bool KGLOBAL>
-__device__ __forceinline__ void jk_ket_class(const JKArgs& a, const BraStage& st, int spos, double* Jt, double* Ksm) {
+__device__ __forceinline__ void jk_ket_class(const JKArgs& a, const BraStage& st, int spos, double* Jt, double* Ksm,
+                                             KetQueue& kq, int& rot) {
     using Q = QClass<CX, CY>;
+    const double q1 = a.q.sortedQ[spos];
+    const double* bm = a.bmax;
+    const int nb = a.nblock;
     for (int sub = 0; sub < NSUB; ++sub) {
         const int seg = CY * NSUB + sub;
         const int64_t cnt = a.q.counts[(size_t)seg * (a.q.npair + 1) + spos];
         if (cnt == 0) continue;
-        const int j0 = a.q.seg_start[seg];
-        const int64_t items = cnt * Q::NCD * Q::NKG;
-        for (int64_t it = threadIdx.x; it < items; it += blockDim.x) {
-            const int kg = static_cast<int>(it % Q::NKG);
-            const int jj = static_cast<int>(it / (Q::NCD * Q::NKG)), cd = static_cast<int>((it / Q::NKG) % Q::NCD);
-            const int P2 = a.q.sorted[j0 + jj];
+        // difference densities: density-weighted test on the six block pairs
+        auto keep = [&](int pos) {
+            if (!bm) return true;
+            const int P2 = a.q.sorted[pos];
             const int C = a.q.pv.pa_blk[P2], Dd = a.q.pv.pb_blk[P2];
-            if (a.bmax) {
-                const double* bm = a.bmax;
-                const int nb = a.nblock;
-                double dm = fmax(fmax(bm[st.A * nb + st.B], bm[C * nb + Dd]),
-                                 fmax(fmax(bm[st.A * nb + C], bm[st.A * nb + Dd]), fmax(bm[st.B * nb + C], bm[st.B * nb + Dd])));
-                if (a.q.sortedQ[spos] * a.q.sortedQ[j0 + jj] * dm < a.dthr) continue;
-            }
+            const double dm = fmax(fmax(bm[st.A * nb + st.B], bm[C * nb + Dd]),
+                                   fmax(fmax(bm[st.A * nb + C], bm[st.A * nb + Dd]),
+                                        fmax(bm[st.B * nb + C], bm[st.B * nb + Dd])));
+            return q1 * a.q.sortedQ[pos] * dm >= a.dthr;
+        };
+        auto work = [&](int pos, int r) {
+            const int kg = r % Q::NKG, cd = r / Q::NKG;
+            const int P2 = a.q.sorted[pos];
+            const int C = a.q.pv.pa_blk[P2], Dd = a.q.pv.pb_blk[P2];
             const int ic = cd / Q::ND, id = cd % Q::ND;
             double v[Q::NROW][Q::KG];
             eri_column<CX, CY>(st, a.q.pv.rec + a.q.pv.slot[P2] * PPW, a.q.pv.npp[P2], ic, id, kg, v);
             jk_digest_column<CX, CY, NS, KGLOBAL>(a, st, P2, C, Dd, ic, id, kg, v, Jt, Ksm);
-        }
+        };
+        ket_items<Q::NCD * Q::NKG>(a.q.seg_start[seg], cnt, kq, rot, keep, work);
     }
 }
 
@@ -433,6 +477,7 @@ __global__ void __launch_bounds__(JK_THREADS) jk_bra_kernel(JKArgs a) {
     const int spos = a.q.cls_start[CX] + (int)(blockIdx.x / KK::NY);
     const int P1 = a.q.sorted[spos];
     __shared__ BraStage st;
+    __shared__ KetQueue kq;
     __shared__ int any;
     if (threadIdx.x == 0) {
         load_stage(a.q, P1, st, Esm);
@@ -448,12 +493,13 @@ __global__ void __launch_bounds__(JK_THREADS) jk_bra_kernel(JKArgs a) {
     stage_bra_e<Q0::LA, Q0::LB, 0>(st);
     __syncthreads();
     constexpr bool KG_ = KK::KGLOBAL;
-    if (yk < 0 || yk == 0) jk_ket_class<CX, 0, NS, KG_>(a, st, spos, Jt, Ksm);
-    if constexpr (CX >= 1) if (yk < 0 || yk == 1) jk_ket_class<CX, 1, NS, KG_>(a, st, spos, Jt, Ksm);
-    if constexpr (CX >= 2) if (yk < 0 || yk == 2) jk_ket_class<CX, 2, NS, KG_>(a, st, spos, Jt, Ksm);
-    if constexpr (CX >= 3) if (yk < 0 || yk == 3) jk_ket_class<CX, 3, NS, KG_>(a, st, spos, Jt, Ksm);
-    if constexpr (CX >= 4) if (yk < 0 || yk == 4) jk_ket_class<CX, 4, NS, KG_>(a, st, spos, Jt, Ksm);
-    if constexpr (CX >= 5) if (yk < 0 || yk == 5) jk_ket_class<CX, 5, NS, KG_>(a, st, spos, Jt, Ksm);
+    int rot = 0;
+    if (yk < 0 || yk == 0) jk_ket_class<CX, 0, NS, KG_>(a, st, spos, Jt, Ksm, kq, rot);
+    if constexpr (CX >= 1) if (yk < 0 || yk == 1) jk_ket_class<CX, 1, NS, KG_>(a, st, spos, Jt, Ksm, kq, rot);
+    if constexpr (CX >= 2) if (yk < 0 || yk == 2) jk_ket_class<CX, 2, NS, KG_>(a, st, spos, Jt, Ksm, kq, rot);
+    if constexpr (CX >= 3) if (yk < 0 || yk == 3) jk_ket_class<CX, 3, NS, KG_>(a, st, spos, Jt, Ksm, kq, rot);
+    if constexpr (CX >= 4) if (yk < 0 || yk == 4) jk_ket_class<CX, 4, NS, KG_>(a, st, spos, Jt, Ksm, kq, rot);
+    if constexpr (CX >= 5) if (yk < 0 || yk == 5) jk_ket_class<CX, 5, NS, KG_>(a, st, spos, Jt, Ksm, kq, rot);
     __syncthreads();
     const size_t nn = (size_t)n * n;
     // flush J_ab: one thread per (set, row) sums the per-thread slots

@@ -27,6 +27,9 @@ struct GradArgs {
     double thr;             // exact screening threshold on Q1 Q2 max|Gamma|
     double* grad;           // [natm][3]
     int natm;
+    const double* bmc;      // [nblock][nblock] max |Dc| per block pair
+    const double* bmx;      // [nblock][nblock] max over x of |Dx| per block pair (nx > 0)
+    int nblock;
 };
 
 // For runtime (i, j): row[t] = E^{ij}_t and drow[t] = 2c E^{i+1,j}_t - i E^{i-1,j}_t
@@ -256,22 +259,37 @@ __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStage& s
     }
 }
 
+// Ket pairs pass the queue when the block bound of Gamma over the whole
+// block quartet, deg [|Dc|_AB |Dc|_CD + |k|/2 nx (|Dx|_AC |Dx|_BD +
+// |Dx|_AD |Dx|_BC)] >= max|Gamma|, can reach the threshold and the quartet
+// is not one-centre; the exact per-column test follows in grad_column.
 template <int CX, int CY>
 __device__ __forceinline__ void grad_ket_class(const GradArgs& a, const BraStage& st, int spos, double (&gab)[6],
-                                               double* gsh) {
+                                               double* gsh, KetQueue& kq, int& rot) {
     using Q = QClass<CX, CY>;
     const double q1 = a.q.sortedQ[spos];
+    const int nb = a.nblock;
+    const double xf = 0.5 * fabs(a.kfac) * a.nx;
     for (int sub = 0; sub < NSUB; ++sub) {
         const int seg = CY * NSUB + sub;
         const int64_t cnt = a.q.counts[(size_t)seg * (a.q.npair + 1) + spos];
         if (cnt == 0) continue;
-        const int j0 = a.q.seg_start[seg];
-        for (int64_t it = threadIdx.x; it < cnt * Q::NCD * Q::NKG; it += blockDim.x) {
-            const int kg = static_cast<int>(it % Q::NKG);
-            const int jj = static_cast<int>(it / (Q::NCD * Q::NKG)), cd = static_cast<int>((it / Q::NKG) % Q::NCD);
-            const int P2 = a.q.sorted[j0 + jj];
-            grad_column<CX, CY>(a, st, P2, q1 * a.q.sortedQ[j0 + jj], cd / Q::ND, cd % Q::ND, kg, gab, gsh);
-        }
+        auto keep = [&](int pos) {
+            const int P2 = a.q.sorted[pos];
+            const int C = a.q.pv.pa_blk[P2], Dd = a.q.pv.pb_blk[P2];
+            const int aC = a.q.bv.atom[C], aD = a.q.bv.atom[Dd];
+            if (st.aA == st.aB && st.aB == aC && aC == aD) return false;
+            double gb = a.bmc[st.A * nb + st.B] * a.bmc[C * nb + Dd];
+            if (a.nx > 0)
+                gb += xf * (a.bmx[st.A * nb + C] * a.bmx[st.B * nb + Dd] + a.bmx[st.A * nb + Dd] * a.bmx[st.B * nb + C]);
+            const double deg = 0.5 * (st.A != st.B ? 2.0 : 1.0) * (C != Dd ? 2.0 : 1.0) * (st.P1 != P2 ? 2.0 : 1.0);
+            return q1 * a.q.sortedQ[pos] * deg * gb >= a.thr;
+        };
+        auto work = [&](int pos, int r) {
+            const int kg = r % Q::NKG, cd = r / Q::NKG;
+            grad_column<CX, CY>(a, st, a.q.sorted[pos], q1 * a.q.sortedQ[pos], cd / Q::ND, cd % Q::ND, kg, gab, gsh);
+        };
+        ket_items<Q::NCD * Q::NKG>(a.q.seg_start[seg], cnt, kq, rot, keep, work);
     }
 }
 
@@ -285,6 +303,7 @@ __global__ void __launch_bounds__(128) grad2e_bra_kernel(GradArgs a) {
     double* gsh = smem;
     double* Esm = smem + 3 * a.natm;
     __shared__ BraStage st;
+    __shared__ KetQueue kq;
     __shared__ int any;
     const int spos = a.q.cls_start[CX] + blockIdx.x;
     if (threadIdx.x == 0) {
@@ -299,7 +318,8 @@ __global__ void __launch_bounds__(128) grad2e_bra_kernel(GradArgs a) {
     stage_bra_e<Q0::LA, Q0::LB, 1>(st);
     __syncthreads();
     double gab[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    grad_ket_class<CX, CY>(a, st, spos, gab, gsh);
+    int rot = 0;
+    grad_ket_class<CX, CY>(a, st, spos, gab, gsh, kq, rot);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         if (gab[d] != 0.0) atomicAdd(gsh + 3 * st.aA + d, gab[d]);

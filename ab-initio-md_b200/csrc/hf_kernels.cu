@@ -70,6 +70,8 @@ struct aimd_ctx {
     int64_t* counts_d;      // difference-density builds (threshold changes every call)
     double* bmax;           // [nblock][nblock] max |D| per block pair
     double* dmax;           // [1] max over bmax
+    double* bmc;            // gradient: [nblock][nblock] max |Dc| and max over x of |Dx|
+    double* bmx;
     cudaStream_t cls_stream[NCLS];
     cudaEvent_t ev_fork, ev_join[NCLS];
     int maxbp[NCLS];        // largest primitive-pair count of a block pair, per class
@@ -210,6 +212,8 @@ extern "C" int aimd_create(aimd_ctx** out, int natm, int nao, int nblock, const 
         CK(dalloc(&c->counts_d, (size_t)NSEG * (np + 1)));
         CK(dalloc(&c->bmax, (size_t)nblock * nblock));
         CK(dalloc(&c->dmax, 1));
+        CK(dalloc(&c->bmc, (size_t)nblock * nblock));
+        CK(dalloc(&c->bmx, (size_t)nblock * nblock));
         for (int cl = 0; cl < NCLS; ++cl) c->maxbp[cl] = 1;
         for (int p = 0; p < np; ++p)
             c->maxbp[cls[p]] = std::max(c->maxbp[cls[p]], blk_np[pa[p]] * blk_np[pb[p]]);
@@ -234,7 +238,7 @@ extern "C" int aimd_destroy(aimd_ctx* c) {
                     c->sh_atom, c->sh_l, c->sh_ao, c->sh_p0, c->sh_np, c->sp_i, c->sp_j, c->sh_exp, c->sh_coef,
                     c->charges, c->pa, c->pb, c->npp, c->slot, c->rec, c->Q, c->by_class, c->idx_in,
                     c->tmp_idx, c->seg_id, c->seg_keys, c->seg_keys_out, c->seg_start, c->tmpQ, c->sortedQ,
-                    c->sorted, c->counts_jk, c->counts_g, c->counts_d, c->bmax, c->dmax, c->cub_tmp, c->pos};
+                    c->sorted, c->counts_jk, c->counts_g, c->counts_d, c->bmax, c->dmax, c->bmc, c->bmx, c->cub_tmp, c->pos};
     for (void* p : ptrs) cudaFree(p);
     for (int i = 0; i < NCLS; ++i) {
         if (c->cls_stream[i]) cudaStreamDestroy(c->cls_stream[i]);
@@ -748,6 +752,16 @@ extern "C" int aimd_grad2e(aimd_ctx* c, const double* Dc, int nx, const double* 
         c->thr_g = thr_enum;
     }
     CK(cudaMemsetAsync(grad, 0, sizeof(double) * 3 * c->natm, st));
+    const int nb2 = c->nblock * c->nblock;
+    block_dmax_kernel<<<(nb2 + 127) / 128, 128, 0, st>>>(c->nblock, c->nao, 1, c->blk_l, c->blk_ncon, c->blk_ao, Dc,
+                                                         c->bmc);
+    ++c->launches;
+    if (nx > 0) {
+        block_dmax_kernel<<<(nb2 + 127) / 128, 128, 0, st>>>(c->nblock, c->nao, nx, c->blk_l, c->blk_ncon, c->blk_ao,
+                                                             Dx, c->bmx);
+        ++c->launches;
+    }
+    CK(cudaGetLastError());
     GradArgs a;
     a.q = quartet_args(c, c->counts_g);
     a.Dc = Dc;
@@ -757,6 +771,9 @@ extern "C" int aimd_grad2e(aimd_ctx* c, const double* Dc, int nx, const double* 
     a.thr = thr;
     a.grad = grad;
     a.natm = c->natm;
+    a.bmc = c->bmc;
+    a.bmx = c->bmx;
+    a.nblock = c->nblock;
     const LaunchEnv e = launch_env(c);
 #define AIMD_GRAD(X, S) launch_grad_class<X>(e, a, S)
     AIMD_EACH_CLASS_CONCURRENT(AIMD_GRAD, "aimd_grad2e");
