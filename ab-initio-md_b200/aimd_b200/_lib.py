@@ -31,6 +31,7 @@ SIGNATURES = {
     "aimd_set_geometry": (_i, [_vp, _vp, _vp]),
     "aimd_schwarz": (_i, [_vp, _vp, _vp]),
     "aimd_pair_count": (_i, [_vp]),
+    "aimd_set_fp32_cutoff": (_i, [_vp, _d]),
     "aimd_jk": (_i, [_vp, _i, _vp, _vp, _vp, _d, _vp]),
     "aimd_jk_delta": (_i, [_vp, _i, _vp, _vp, _vp, _d, _d, _vp]),
     "aimd_eri_tensor": (_i, [_vp, _vp, _d, _vp]),

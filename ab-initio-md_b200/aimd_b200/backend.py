@@ -200,7 +200,8 @@ class HFGPUBackend(ForceBackend):
         self._guess = None
         res = self.solver.run(x, guess=guess)
         t1 = time.perf_counter()
-        gradient = scf_gradient(res, schwarz_threshold=self.gradient_screening)
+        gradient = scf_gradient(res, schwarz_threshold=self.gradient_screening,
+                                fp32_cutoff=self.solver.options.fp32_cutoff)
         t2 = time.perf_counter()
         density = res.guess_density
         if self.reuse_density:
@@ -222,6 +223,7 @@ class HFGPUBackend(ForceBackend):
             "commutator_norm": float(res.commutator_norm), "s2": float(res.s2), "s2_exact": float(res.s2_exact),
             "mulliken_charges": res.mulliken_charges.copy(), "guess": label, "init_guess": self.init_guess,
             "n_removed": int(res.n_removed), "warnings": warnings_,
+            "fp32_cutoff": float(self.solver.options.fp32_cutoff),
             "timings": {"integrals": float(res.timings.get("integrals", 0.0)),
                         "guess": float(res.timings.get("guess", 0.0)),
                         "scf_iterations": float(res.timings.get("iterations", 0.0)),

@@ -32,12 +32,18 @@ FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std
 
 
 def _units() -> list[tuple[str, str, list[str]]]:
-    units = [(os.path.join(CSRC, "hf_class_jk.cu"), os.path.join(OBJ_DIR, f"hf_class_jk_{x}.o"),
-              [f"-DAIMD_CLASS={x}"]) for x in range(6)]
-    units += [(os.path.join(CSRC, "hf_class_grad.cu"), os.path.join(OBJ_DIR, f"hf_class_grad_{x}_{y}.o"),
-               [f"-DAIMD_CLASS={x}", f"-DAIMD_KET={y}"]) for x in range(6) for y in range(x + 1)]
-    # slowest units first so the parallel build finishes sooner
-    units.sort(key=lambda u: -sum(int(f.split("=")[1]) for f in u[2]))
+    # one unit per class (and ket class) and arithmetic type (0 FP64, 1 FP32)
+    units = [(os.path.join(CSRC, "hf_class_jk.cu"), os.path.join(OBJ_DIR, f"hf_class_jk_{x}_r{r}.o"),
+              [f"-DAIMD_CLASS={x}", f"-DAIMD_REAL={r}"]) for x in range(6) for r in (0, 1)]
+    units += [(os.path.join(CSRC, "hf_class_grad.cu"), os.path.join(OBJ_DIR, f"hf_class_grad_{x}_{y}_r{r}.o"),
+               [f"-DAIMD_CLASS={x}", f"-DAIMD_KET={y}", f"-DAIMD_REAL={r}"])
+              for x in range(6) for y in range(x + 1) for r in (0, 1)]
+    # slowest units first so the parallel build finishes sooner (a J/K unit
+    # of class X takes about as long as the gradient units of (X, X))
+    def cost(u):
+        v = [int(f.split("=")[1]) for f in u[2]]
+        return 2 * v[0] + 1 if "hf_class_jk" in u[0] else v[0] + v[1]
+    units.sort(key=lambda u: -cost(u))
     units.append((os.path.join(CSRC, "hf_onee.cu"), os.path.join(OBJ_DIR, "hf_onee.o"), []))
     units.append((os.path.join(CSRC, "hf_kernels.cu"), os.path.join(OBJ_DIR, "hf_kernels.o"), []))
     return units

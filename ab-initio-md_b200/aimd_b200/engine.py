@@ -108,6 +108,14 @@ class Engine:
         self.npair = self.lib.aimd_pair_count(h)
         self._pos_key: bytes | None = None
         self.pos = torch.zeros((self.natm, 3), dtype=torch.float64, device=self.device)
+        self._fp32_cutoff = 0.0
+
+    def _precision(self, fp32_cutoff: float) -> None:
+        """Quartets with Q1 Q2 < fp32_cutoff run in FP32 in the next calls (0: all FP64)."""
+        c = float(fp32_cutoff)
+        if c != self._fp32_cutoff:
+            _lib.check(self.lib.aimd_set_fp32_cutoff(self.handle, c), "aimd_set_fp32_cutoff")
+            self._fp32_cutoff = c
 
     def __del__(self) -> None:
         h = getattr(self, "handle", None)
@@ -141,8 +149,9 @@ class Engine:
         _lib.check(self.lib.aimd_schwarz(self.handle, ctypes.c_void_p(Q.data_ptr()), _stream()), "aimd_schwarz")
         return Q
 
-    def jk_acc(self, D: torch.Tensor, thr: float) -> tuple[torch.Tensor, torch.Tensor]:
+    def jk_acc(self, D: torch.Tensor, thr: float, fp32_cutoff: float = 0.0) -> tuple[torch.Tensor, torch.Tensor]:
         """Un-symmetrised J/K accumulators for symmetric densities D[nset, n, n]."""
+        self._precision(fp32_cutoff)
         D = D.contiguous()
         J = torch.empty_like(D)
         K = torch.empty_like(D)
@@ -151,8 +160,10 @@ class Engine:
                                     _stream()), "aimd_jk")
         return J, K
 
-    def jk_delta_acc(self, dD: torch.Tensor, thr: float, dthr: float) -> tuple[torch.Tensor, torch.Tensor]:
+    def jk_delta_acc(self, dD: torch.Tensor, thr: float, dthr: float,
+                     fp32_cutoff: float = 0.0) -> tuple[torch.Tensor, torch.Tensor]:
         """Accumulators of J/K for difference densities with density-weighted screening."""
+        self._precision(fp32_cutoff)
         dD = dD.contiguous()
         J = torch.empty_like(dD)
         K = torch.empty_like(dD)
@@ -162,13 +173,16 @@ class Engine:
         return J, K
 
     def eri_tensor(self, thr: float) -> torch.Tensor:
+        self._precision(0.0)
         n = self.nao
         eri = torch.empty((n, n, n, n), dtype=torch.float64, device=self.device)
         _lib.check(self.lib.aimd_eri_tensor(self.handle, ctypes.c_void_p(eri.data_ptr()), float(thr), _stream()),
                    "aimd_eri_tensor")
         return eri
 
-    def grad2e(self, Dc: torch.Tensor, Dx: torch.Tensor, kfac: float, thr: float, gamma_bound: float) -> torch.Tensor:
+    def grad2e(self, Dc: torch.Tensor, Dx: torch.Tensor, kfac: float, thr: float, gamma_bound: float,
+               fp32_cutoff: float = 0.0) -> torch.Tensor:
+        self._precision(fp32_cutoff)
         Dc = Dc.contiguous()
         Dx = Dx.contiguous()
         g = torch.empty((self.natm, 3), dtype=torch.float64, device=self.device)

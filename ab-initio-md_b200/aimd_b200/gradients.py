@@ -59,7 +59,7 @@ def _check(result: SCFResult, require_converged: bool) -> None:
                          f"{result.commutator_norm:.2e}); its analytic gradient is not dE/dR")
 
 
-def _device_terms(result: SCFResult, schwarz_threshold: float):
+def _device_terms(result: SCFResult, schwarz_threshold: float, fp32_cutoff: float = 0.0):
     b = result.basis
     dev = result.device
     if dev:
@@ -75,12 +75,16 @@ def _device_terms(result: SCFResult, schwarz_threshold: float):
         Dx, k = spin, 1.0
     else:
         Dx, k = P[None], 0.5
-    g2 = I.two_electron_gradient_device(b, P, Dx.contiguous(), k, schwarz_threshold)
+    g2 = I.two_electron_gradient_device(b, P, Dx.contiguous(), k, schwarz_threshold, fp32_cutoff)
     return g1, g2
 
 
-def scf_gradient_device(state, schwarz_threshold: float = I.DEFAULT_SCHWARZ_GRAD) -> torch.Tensor:
-    """Analytic gradient of a DeviceSCFState as a device tensor (nuclear term included)."""
+def scf_gradient_device(state, schwarz_threshold: float = I.DEFAULT_SCHWARZ_GRAD,
+                        fp32_cutoff: float = 0.0) -> torch.Tensor:
+    """
+    Analytic gradient of a DeviceSCFState as a device tensor (nuclear term
+    included); quartets with Q1 Q2 < fp32_cutoff in FP32 (0: all FP64).
+    """
     b = state.basis
     spin, F = state.spin, state.fock
     P = spin[0] + spin[1]
@@ -90,17 +94,22 @@ def scf_gradient_device(state, schwarz_threshold: float = I.DEFAULT_SCHWARZ_GRAD
         Dx, k = spin, 1.0
     else:
         Dx, k = P[None], 0.5
-    g = g + I.two_electron_gradient_device(b, P, Dx.contiguous(), k, schwarz_threshold)
+    g = g + I.two_electron_gradient_device(b, P, Dx.contiguous(), k, schwarz_threshold, fp32_cutoff)
     gn = torch.as_tensor(I.nuclear_repulsion_gradient(b.nuclear_charges, b.positions), device=g.device)
     return g + gn
 
 
 def scf_gradient(result: SCFResult, schwarz_threshold: float = I.DEFAULT_SCHWARZ_GRAD,
-                 require_converged: bool = False, blas_threads: int | None = 1) -> np.ndarray:
-    """Analytic dE/dR (Eh/bohr, (natm, 3)) of an RHF or UHF SCF result (aimd/qc/gradients.py:168-193)."""
+                 require_converged: bool = False, blas_threads: int | None = 1,
+                 fp32_cutoff: float = 0.0) -> np.ndarray:
+    """
+    Analytic dE/dR (Eh/bohr, (natm, 3)) of an RHF or UHF SCF result
+    (aimd/qc/gradients.py:168-193); ``fp32_cutoff`` > 0 evaluates the
+    two-electron quartets with Q1 Q2 below it in FP32 (mixed precision).
+    """
     _check(result, require_converged)
     b = result.basis
-    g1, g2 = _device_terms(result, schwarz_threshold)
+    g1, g2 = _device_terms(result, schwarz_threshold, fp32_cutoff)
     g = I.nuclear_repulsion_gradient(b.nuclear_charges, b.positions)
     return g + (g1 + g2).cpu().numpy()
 

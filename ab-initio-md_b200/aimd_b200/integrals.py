@@ -71,20 +71,21 @@ def jk_from_eri(eri, densities):
 
 
 def jk_device(basis: BasisSet, D: torch.Tensor, schwarz_threshold: float = DEFAULT_SCHWARZ,
-              symmetric: bool | None = None) -> tuple[torch.Tensor, torch.Tensor]:
+              symmetric: bool | None = None, fp32_cutoff: float = 0.0) -> tuple[torch.Tensor, torch.Tensor]:
     """
     Integral-direct J, K for a stack D[nset, n, n] (CUDA float64). Symmetric
     densities take one pass; otherwise J uses the symmetric part and
-    K = A(D) + A(D^T)^T from a pass over [D, D^T].
+    K = A(D) + A(D^T)^T from a pass over [D, D^T]. Quartets with
+    Q1 Q2 < fp32_cutoff are evaluated in FP32 (0: all FP64).
     """
     eng = engine_for(basis)
     if symmetric is None:
         symmetric = bool(torch.equal(D, D.transpose(1, 2)))
     if symmetric:
-        Ja, Ka = eng.jk_acc(D, schwarz_threshold)
+        Ja, Ka = eng.jk_acc(D, schwarz_threshold, fp32_cutoff)
         return Ja + Ja.transpose(1, 2), Ka + Ka.transpose(1, 2)
     m = D.shape[0]
-    Ja, Ka = eng.jk_acc(torch.cat([D, D.transpose(1, 2)]).contiguous(), schwarz_threshold)
+    Ja, Ka = eng.jk_acc(torch.cat([D, D.transpose(1, 2)]).contiguous(), schwarz_threshold, fp32_cutoff)
     Jh = Ja + Ja.transpose(1, 2)
     return 0.5 * (Jh[:m] + Jh[m:]), Ka[:m] + Ka[m:].transpose(1, 2)
 
@@ -106,10 +107,11 @@ def gamma_bound(Dc: torch.Tensor, Dx: torch.Tensor, k_factor: float) -> float:
 
 
 def two_electron_gradient_device(basis: BasisSet, Dc: torch.Tensor, Dx: torch.Tensor, k_factor: float,
-                                 schwarz_threshold: float = DEFAULT_SCHWARZ_GRAD) -> torch.Tensor:
+                                 schwarz_threshold: float = DEFAULT_SCHWARZ_GRAD,
+                                 fp32_cutoff: float = 0.0) -> torch.Tensor:
     """d/dR of 1/2 sum Gamma (mn|ls) at fixed symmetric densities, (natm, 3) on the device."""
     eng = engine_for(basis)
-    return eng.grad2e(Dc, Dx, k_factor, schwarz_threshold, gamma_bound(Dc, Dx, k_factor))
+    return eng.grad2e(Dc, Dx, k_factor, schwarz_threshold, gamma_bound(Dc, Dx, k_factor), fp32_cutoff)
 
 
 def two_electron_gradient(basis: BasisSet, D_coulomb, D_exchange_list: Sequence, k_factor: float,

@@ -152,10 +152,11 @@ class DeviceXLBOMD:
         self.dt = timestep_fs * FS_TO_AU_TIME
         self.thermo = thermostat
         self.thr = gradient_screening
+        self.fp32_cutoff = solver.options.fp32_cutoff
         kappa, alpha, c = XL_COEFFICIENTS[k]
         self.kappa, self.alpha, self.c = kappa, alpha, [float(v) for v in c]
         self.state = self._run(solver, self.x, None)
-        self.gradient = self._grad(self.state, self.thr)
+        self.gradient = self._grad(self.state, self.thr, self.fp32_cutoff)
         D = self._density(self.state)
         self.history = [D.clone() for _ in range(k + 1)]
         self.iterations = [self.state.iterations]
@@ -178,7 +179,7 @@ class DeviceXLBOMD:
         guess = 2.0 * h[0] - h[1] + self.kappa * (D - h[0]) + self.alpha * diss
         self.history = [guess] + h[:-1]
         self.state = self._run(self.solver, self.x, guess)
-        self.gradient = self._grad(self.state, self.thr)
+        self.gradient = self._grad(self.state, self.thr, self.fp32_cutoff)
         acc = -self.gradient.cpu().numpy() / self.m[:, None]
         self.v += 0.5 * dt * acc
         if self.thermo is not None:

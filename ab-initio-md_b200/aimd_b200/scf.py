@@ -67,6 +67,9 @@ class SCFOptions:
     # delta_threshold None: min(schwarz_threshold, 1e-3 conv_energy), which
     # keeps the accumulated screening error of the energy well below
     # conv_energy (measured ~300 delta_threshold on methanol 6-31G**)
+    # mixed precision: ERI quartets with Schwarz product Q1 Q2 below
+    # fp32_cutoff are evaluated in FP32, with FP64 accumulation (0: plain FP64)
+    fp32_cutoff: float = 0.0
     incremental_fock: bool = True
     fock_rebuild: int = 10
     delta_threshold: float | None = None
@@ -92,6 +95,8 @@ class SCFOptions:
             raise ValueError("lindep_threshold must be positive")
         if self.blas_threads is not None and self.blas_threads < 1:
             raise ValueError("blas_threads must be >= 1 or None")
+        if not (self.fp32_cutoff >= 0.0 and np.isfinite(self.fp32_cutoff)):
+            raise ValueError("fp32_cutoff must be finite and >= 0")
         if self.fock_rebuild < 1:
             raise ValueError("fock_rebuild must be >= 1")
         if self.delta_threshold is not None and not self.delta_threshold > 0.0:
@@ -614,12 +619,12 @@ class SCFSolver:
         if inc is not None and inc.get("D") is not None and inc["n"] < opt.fock_rebuild:
             from .engine import engine_for
             Ja, Ka = engine_for(Ik.basis).jk_delta_acc((Ds - inc["D"]).contiguous(), opt.schwarz_threshold,
-                                                       opt.fock_delta_threshold)
+                                                       opt.fock_delta_threshold, opt.fp32_cutoff)
             J = inc["J"] + Ja + Ja.transpose(1, 2)
             K = inc["K"] + Ka + Ka.transpose(1, 2)
             inc["n"] += 1
         else:
-            J, K = I.jk_device(Ik.basis, Ds, opt.schwarz_threshold, symmetric=True)
+            J, K = I.jk_device(Ik.basis, Ds, opt.schwarz_threshold, symmetric=True, fp32_cutoff=opt.fp32_cutoff)
             if inc is not None:
                 inc["n"] = 1
         if inc is not None:

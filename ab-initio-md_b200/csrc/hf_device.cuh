@@ -108,12 +108,32 @@ __device__ __forceinline__ double boys_top(double x, double ex) {
     return f;
 }
 
-// R_tuv(alpha, PQ) for all t+u+v <= L, in place: levels n = L..0, each level
-// overwriting the previous one in decreasing Hermite index (entries h only
-// read lower indices of the level above). R[0] of level n is (-2a)^n F_n.
+// FP32 F_N(x) for x < 40 (the mixed-precision quartets): the same series
+// with 16 + N terms (relative truncation < 2e-8 at x = N + 1.5), or erf and
+// the upward recursion above N + 1.5.
+template <int N>
+__device__ __forceinline__ float boys_top_f(float x, float ex) {
+    if (x < N + 1.5f) {
+        constexpr int NT = 16 + N;
+        const float y = 2.0f * x;
+        float s = static_cast<float>(boys_series_coef(N, NT - 1));
+#pragma unroll
+        for (int k = NT - 2; k >= 0; --k) s = fmaf(s, y, static_cast<float>(boys_series_coef(N, k)));
+        return ex * s;
+    }
+    const float sx = sqrtf(x);
+    float f = 0.886226925f * erff(sx) / sx;
+    if (N > 0) {
+        const float inv2x = 0.5f / x;
+#pragma unroll
+        for (int m = 0; m < N; ++m) f = ((2 * m + 1) * f - ex) * inv2x;
+    }
+    return f;
+}
+
+// g[n] = (-2 alpha)^n F_n(T), n = 0..L: the level seeds of hermite_r.
 template <int L>
-__device__ __forceinline__ void hermite_r(double alpha, double X, double Y, double Z, double (&R)[nherm(L)]) {
-    const double T = alpha * (X * X + Y * Y + Z * Z);
+__device__ __forceinline__ void boys_scaled(double alpha, double T, double (&g)[L + 1]) {
     const double ex = exp(-T);
     double f = boys_top<L>(T, ex);
     const double m2a = -2.0 * alpha;
@@ -121,10 +141,57 @@ __device__ __forceinline__ void hermite_r(double alpha, double X, double Y, doub
     pw[0] = 1.0;
 #pragma unroll
     for (int n = 1; n <= L; ++n) pw[n] = pw[n - 1] * m2a;
-    R[0] = pw[L] * f;
+    g[L] = pw[L] * f;
 #pragma unroll
     for (int n = L - 1; n >= 0; --n) {
         f = (2.0 * T * f + ex) * (1.0 / (2 * n + 1));
+        g[n] = pw[n] * f;
+    }
+}
+// FP32 quartets: below T = 40 in FP32; from T = 40 on (where F_n(T) alone
+// can leave the FP32 range) in FP64, in the asymptotic form
+// (-2a)^n F_n = (-a/T)^n (2n-1)!! F_0, F_0 = sqrt(pi/T)/2, e^-T < 5e-18.
+template <int L>
+__device__ __forceinline__ void boys_scaled(float alpha, float T, float (&g)[L + 1]) {
+    if (T >= 40.0f) {
+        const double td = T;
+        double gn = 0.88622692545275801365 / sqrt(td);
+        const double s = -static_cast<double>(alpha) / td;
+        g[0] = static_cast<float>(gn);
+#pragma unroll
+        for (int n = 1; n <= L; ++n) {
+            gn *= (2 * n - 1) * s;
+            g[n] = static_cast<float>(gn);
+        }
+        return;
+    }
+    const float ex = expf(-T);
+    float f = boys_top_f<L>(T, ex);
+    const float m2a = -2.0f * alpha;
+    float pw[L + 1];
+    pw[0] = 1.0f;
+#pragma unroll
+    for (int n = 1; n <= L; ++n) pw[n] = pw[n - 1] * m2a;
+    g[L] = pw[L] * f;
+#pragma unroll
+    for (int n = L - 1; n >= 0; --n) {
+        f = (2.0f * T * f + ex) * (1.0f / (2 * n + 1));
+        g[n] = pw[n] * f;
+    }
+}
+
+// R_tuv(alpha, PQ) for all t+u+v <= L, in place: levels n = L..0, each level
+// overwriting the previous one in decreasing Hermite index (entries h only
+// read lower indices of the level above). R[0] of level n is (-2a)^n F_n.
+// RT = double (plain path) or float (mixed-precision quartets).
+template <int L, typename RT>
+__device__ __forceinline__ void hermite_r(RT alpha, RT X, RT Y, RT Z, RT (&R)[nherm(L)]) {
+    const RT T = alpha * (X * X + Y * Y + Z * Z);
+    RT g[L + 1];
+    boys_scaled<L>(alpha, T, g);
+    R[0] = g[L];
+#pragma unroll
+    for (int n = L - 1; n >= 0; --n) {
         // level n from level n+1; degrees d = L-n .. 1, decreasing index
 #pragma unroll
         for (int d = L - n; d >= 1; --d) {
@@ -133,7 +200,7 @@ __device__ __forceinline__ void hermite_r(double alpha, double X, double Y, doub
 #pragma unroll
                 for (int u = 0; u <= d - t; ++u) {
                     const int v = d - t - u;
-                    double r;
+                    RT r;
                     if (t > 0) {
                         r = X * R[hidx(t - 1, u, v)];
                         if (t > 1) r += (t - 1) * R[hidx(t - 2, u, v)];
@@ -148,27 +215,26 @@ __device__ __forceinline__ void hermite_r(double alpha, double X, double Y, doub
                 }
             }
         }
-        R[0] = pw[n] * f;
+        R[0] = g[n];
     }
 }
 
 // E^{ij}_t for i <= IM, j <= JM, t <= i + j, one direction: e[i][j][t].
 // pa = P - A, pb = P - B, oo2p = 1/(2p), e00 = E^{00}_0.
-template <int IM, int JM>
-__device__ __forceinline__ void hermite_e(double pa, double pb, double oo2p, double e00,
-                                          double (&e)[IM + 1][JM + 1][IM + JM + 1]) {
+template <int IM, int JM, typename RT>
+__device__ __forceinline__ void hermite_e(RT pa, RT pb, RT oo2p, RT e00, RT (&e)[IM + 1][JM + 1][IM + JM + 1]) {
 #pragma unroll
     for (int i = 0; i <= IM; ++i)
 #pragma unroll
         for (int j = 0; j <= JM; ++j)
 #pragma unroll
-            for (int t = 0; t <= IM + JM; ++t) e[i][j][t] = 0.0;
+            for (int t = 0; t <= IM + JM; ++t) e[i][j][t] = RT(0);
     e[0][0][0] = e00;
 #pragma unroll
     for (int j = 1; j <= JM; ++j)
 #pragma unroll
         for (int t = 0; t <= j; ++t) {
-            double v = pb * e[0][j - 1][t];
+            RT v = pb * e[0][j - 1][t];
             if (t + 1 <= j - 1) v += (t + 1) * e[0][j - 1][t + 1];
             if (t > 0) v += oo2p * e[0][j - 1][t - 1];
             e[0][j][t] = v;
@@ -179,7 +245,7 @@ __device__ __forceinline__ void hermite_e(double pa, double pb, double oo2p, dou
         for (int j = 0; j <= JM; ++j)
 #pragma unroll
             for (int t = 0; t <= i + j; ++t) {
-                double v = pa * e[i - 1][j][t];
+                RT v = pa * e[i - 1][j][t];
                 if (t + 1 <= i - 1 + j) v += (t + 1) * e[i - 1][j][t + 1];
                 if (t > 0) v += oo2p * e[i - 1][j][t - 1];
                 e[i][j][t] = v;

@@ -45,19 +45,24 @@ struct BraE {
     __device__ static int at(int d, int i, int j, int t) { return ((d * I + i) * J + j) * T + t; }
 };
 
-// Shared-memory stage of one bra pair.
+// Shared-memory stage of one bra pair. The E tables and per-primitive
+// scalars are held in the arithmetic type RT of the kernel that reads them
+// (double, or float for the mixed-precision quartets); they are computed in
+// FP64 either way.
 constexpr int SBW = 12;     // per bra primitive: p, 1/p, Px, Py, Pz, a, b, -, c0..c3
-struct BraStage {
+template <typename RT>
+struct BraStageT {
     int P1, A, B, nbp, aA, aB;
     int nA, nB, oA, oB;
     const double* rec;      // bra primitive records (global)
-    double* E;              // [nbp][BraE::SIZE] (shared)
-    double* SB;             // [nbp][SBW] (shared)
+    RT* E;                  // [nbp][BraE::SIZE] (shared)
+    RT* SB;                 // [nbp][SBW] (shared)
 };
+using BraStage = BraStageT<double>;
 
 // Fill the shared stage (E tables and scalars) for all bra primitives.
-template <int LA, int LB, int G>
-__device__ __forceinline__ void stage_bra_e(const BraStage& st) {
+template <int LA, int LB, int G, typename RT>
+__device__ __forceinline__ void stage_bra_e(const BraStageT<RT>& st) {
     using BE = BraE<LA, LB, G>;
     for (int w = threadIdx.x; w < st.nbp * 3; w += blockDim.x) {
         const int ib = w / 3, d = w % 3;
@@ -65,57 +70,53 @@ __device__ __forceinline__ void stage_bra_e(const BraStage& st) {
         const double p = b[0] + b[1];
         double e[LA + 1 + G][LB + 1 + G][LA + LB + 1 + 2 * G];
         hermite_e<LA + G, LB + G>(b[6 + d], b[9 + d], 0.5 / p, d == 0 ? b[2] : 1.0, e);
-        double* out = st.E + (size_t)ib * BE::SIZE;
+        RT* out = st.E + (size_t)ib * BE::SIZE;
 #pragma unroll
         for (int i = 0; i < LA + 1 + G; ++i)
 #pragma unroll
             for (int j = 0; j < LB + 1 + G; ++j)
 #pragma unroll
-                for (int t = 0; t < LA + LB + 1 + 2 * G; ++t) out[BE::at(d, i, j, t)] = e[i][j][t];
+                for (int t = 0; t < LA + LB + 1 + 2 * G; ++t) out[BE::at(d, i, j, t)] = static_cast<RT>(e[i][j][t]);
     }
     for (int ib = threadIdx.x; ib < st.nbp; ib += blockDim.x) {
         const double* b = st.rec + (size_t)ib * PPW;
-        double* o = st.SB + (size_t)ib * SBW;
+        RT* o = st.SB + (size_t)ib * SBW;
         const double p = b[0] + b[1];
-        o[0] = p;
-        o[1] = 1.0 / p;
-        o[2] = b[3];
-        o[3] = b[4];
-        o[4] = b[5];
-        o[5] = b[0];
-        o[6] = b[1];
-        o[7] = 0.0;
-        o[8] = b[12];
-        o[9] = b[13];
-        o[10] = b[14];
-        o[11] = b[15];
+        const double vals[SBW] = {p, 1.0 / p, b[3], b[4], b[5], b[0], b[1], 0.0, b[12], b[13], b[14], b[15]};
+#pragma unroll
+        for (int i = 0; i < SBW; ++i) o[i] = static_cast<RT>(vals[i]);
     }
 }
 
 // One primitive-pair record of a ket pair (16 doubles, 128-byte aligned),
-// loaded with 16-byte vector loads.
-struct KetRec {
-    double a, b, K, Qx, Qy, Qz, QAx, QAy, QAz, QBx, QBy, QBz, c[4];
+// loaded with 16-byte vector loads, held in the kernel's arithmetic type.
+template <typename RT>
+struct KetRecT {
+    RT a, b, K, Qx, Qy, Qz, QAx, QAy, QAz, QBx, QBy, QBz, c[4];
 };
-__device__ __forceinline__ KetRec load_ket(const double* __restrict__ rec) {
+template <typename RT>
+__device__ __forceinline__ KetRecT<RT> load_ket(const double* __restrict__ rec) {
     const double2* r2 = reinterpret_cast<const double2*>(rec);
-    KetRec k;
-    double2 v = __ldg(r2 + 0); k.a = v.x; k.b = v.y;
-    v = __ldg(r2 + 1); k.K = v.x; k.Qx = v.y;
-    v = __ldg(r2 + 2); k.Qy = v.x; k.Qz = v.y;
-    v = __ldg(r2 + 3); k.QAx = v.x; k.QAy = v.y;
-    v = __ldg(r2 + 4); k.QAz = v.x; k.QBx = v.y;
-    v = __ldg(r2 + 5); k.QBy = v.x; k.QBz = v.y;
-    v = __ldg(r2 + 6); k.c[0] = v.x; k.c[1] = v.y;
-    v = __ldg(r2 + 7); k.c[2] = v.x; k.c[3] = v.y;
+    KetRecT<RT> k;
+    double2 v = __ldg(r2 + 0); k.a = (RT)v.x; k.b = (RT)v.y;
+    v = __ldg(r2 + 1); k.K = (RT)v.x; k.Qx = (RT)v.y;
+    v = __ldg(r2 + 2); k.Qy = (RT)v.x; k.Qz = (RT)v.y;
+    v = __ldg(r2 + 3); k.QAx = (RT)v.x; k.QAy = (RT)v.y;
+    v = __ldg(r2 + 4); k.QAz = (RT)v.x; k.QBx = (RT)v.y;
+    v = __ldg(r2 + 5); k.QBy = (RT)v.x; k.QBz = (RT)v.y;
+    v = __ldg(r2 + 6); k.c[0] = (RT)v.x; k.c[1] = (RT)v.y;
+    v = __ldg(r2 + 7); k.c[2] = (RT)v.x; k.c[3] = (RT)v.y;
     return k;
 }
 
+__device__ __forceinline__ double rsqrt_t(double x) { return rsqrt(x); }
+__device__ __forceinline__ float rsqrt_t(float x) { return rsqrtf(x); }
+
 // out[t] = e[i][j][t] for runtime (i, j), by predicated copies (no local memory).
-template <int IM, int JM, int T>
-__device__ __forceinline__ void select_row(const double (&e)[IM + 1][JM + 1][T + 1], int i, int j, double (&out)[T + 1]) {
+template <int IM, int JM, int T, typename RT>
+__device__ __forceinline__ void select_row(const RT (&e)[IM + 1][JM + 1][T + 1], int i, int j, RT (&out)[T + 1]) {
 #pragma unroll
-    for (int t = 0; t <= T; ++t) out[t] = 0.0;
+    for (int t = 0; t <= T; ++t) out[t] = RT(0);
 #pragma unroll
     for (int ii = 0; ii <= IM; ++ii)
 #pragma unroll
@@ -129,9 +130,9 @@ __device__ __forceinline__ void select_row(const double (&e)[IM + 1][JM + 1][T +
 // ket pair records rk with nkp primitive pairs); r = (ka*KB + kb)*NAB +
 // ia*NB + jb, kk = kc*KD + kd. Ket primitives outermost (each record is read
 // once), bra primitives inner (shared-memory broadcast).
-template <int CX, int CY>
-__device__ __forceinline__ void eri_column(const BraStage& st, const double* __restrict__ rk, int nkp, int ic, int id,
-                                           int kg, double (&v)[QClass<CX, CY>::NROW][QClass<CX, CY>::KG]) {
+template <int CX, int CY, typename RT>
+__device__ __forceinline__ void eri_column(const BraStageT<RT>& st, const double* __restrict__ rk, int nkp, int ic,
+                                           int id, int kg, RT (&v)[QClass<CX, CY>::NROW][QClass<CX, CY>::KG]) {
     using Q = QClass<CX, CY>;
     using BE = BraE<Q::LA, Q::LB, 0>;
     constexpr int LA = Q::LA, LB = Q::LB, LC = Q::LC, LD = Q::LD, LAB = Q::LAB, LCD = Q::LCD, L = Q::L;
@@ -139,61 +140,61 @@ __device__ __forceinline__ void eri_column(const BraStage& st, const double* __r
     constexpr int UH = L >= 6 ? 1 : 16;
     const int cx = cart_x(LC, ic), cy = cart_y(LC, ic), cz = cart_z(LC, ic);
     const int dx = cart_x(LD, id), dy = cart_y(LD, id), dz = cart_z(LD, id);
-    const double fcd = cart_norm(cx, cy, cz) * cart_norm(dx, dy, dz);
+    const RT fcd = static_cast<RT>(cart_norm(cx, cy, cz) * cart_norm(dx, dy, dz));
 #pragma unroll
     for (int r = 0; r < Q::NROW; ++r)
 #pragma unroll
-        for (int k = 0; k < Q::KG; ++k) v[r][k] = 0.0;
+        for (int k = 0; k < Q::KG; ++k) v[r][k] = RT(0);
     for (int ik = 0; ik < nkp; ++ik) {
-        const KetRec k = load_ket(rk + (size_t)ik * PPW);
-        const double q = k.a + k.b, oo2q = 0.5 / q, iq = 2.0 * oo2q;
+        const KetRecT<RT> k = load_ket<RT>(rk + (size_t)ik * PPW);
+        const RT q = k.a + k.b, oo2q = RT(0.5) / q, iq = RT(2) * oo2q;
         // ket E coefficients of this column only (box t2 <= cx+dx, ...)
-        double ex[LCD + 1], ey[LCD + 1], ez[LCD + 1];
+        RT ex[LCD + 1], ey[LCD + 1], ez[LCD + 1];
         {
-            double e[LC + 1][LD + 1][LCD + 1];
+            RT e[LC + 1][LD + 1][LCD + 1];
             hermite_e<LC, LD>(k.QAx, k.QBx, oo2q, k.K, e);
             select_row<LC, LD, LCD>(e, cx, dx, ex);
-            hermite_e<LC, LD>(k.QAy, k.QBy, oo2q, 1.0, e);
+            hermite_e<LC, LD>(k.QAy, k.QBy, oo2q, RT(1), e);
             select_row<LC, LD, LCD>(e, cy, dy, ey);
-            hermite_e<LC, LD>(k.QAz, k.QBz, oo2q, 1.0, e);
+            hermite_e<LC, LD>(k.QAz, k.QBz, oo2q, RT(1), e);
             select_row<LC, LD, LCD>(e, cz, dz, ez);
         }
-        double ck[Q::KG];
+        RT ck[Q::KG];
 #pragma unroll
         for (int i = 0; i < Q::KG; ++i) {
-            double c = k.c[0];
+            RT c = k.c[0];
 #pragma unroll
             for (int j = 1; j < Q::KCD; ++j)
                 if (j == kg * Q::KG + i) c = k.c[j];
             ck[i] = c * fcd;
         }
         for (int ib = 0; ib < st.nbp; ++ib) {
-            const double* sb = st.SB + ib * SBW;
-            const double p = sb[0];
-            const double rs = rsqrt(p + q);
-            const double alpha = p * q * rs * rs;
-            const double pref = TWO_PI_2_5 * sb[1] * iq * rs;
-            double R[nherm(L)];
+            const RT* sb = st.SB + ib * SBW;
+            const RT p = sb[0];
+            const RT rs = rsqrt_t(p + q);
+            const RT alpha = p * q * rs * rs;
+            const RT pref = RT(TWO_PI_2_5) * sb[1] * iq * rs;
+            RT R[nherm(L)];
             hermite_r<L>(alpha, sb[2] - k.Qx, sb[3] - k.Qy, sb[4] - k.Qz, R);
-            double X[Q::NHB];
+            RT X[Q::NHB];
 #pragma unroll UH
             for (int t = 0; t <= LAB; ++t)
 #pragma unroll UH
                 for (int u = 0; u <= LAB - t; ++u)
 #pragma unroll
                     for (int w = 0; w <= LAB - t - u; ++w) {
-                        double s = 0.0;
+                        RT s = RT(0);
 #pragma unroll
                         for (int t2 = 0; t2 <= LCD; ++t2) {
                             if (t2 > cx + dx) continue;
 #pragma unroll
                             for (int u2 = 0; u2 <= LCD; ++u2) {
                                 if (u2 > cy + dy) continue;
-                                const double exy = ((t2 + u2) & 1) ? -ex[t2] * ey[u2] : ex[t2] * ey[u2];
+                                const RT exy = ((t2 + u2) & 1) ? -ex[t2] * ey[u2] : ex[t2] * ey[u2];
 #pragma unroll
                                 for (int v2 = 0; v2 <= LCD; ++v2) {
                                     if (v2 > cz + dz) continue;
-                                    const double e = (v2 & 1) ? -exy * ez[v2] : exy * ez[v2];
+                                    const RT e = (v2 & 1) ? -exy * ez[v2] : exy * ez[v2];
                                     s += e * R[hidx(t + t2, u + u2, w + v2)];
                                 }
                             }
@@ -201,27 +202,27 @@ __device__ __forceinline__ void eri_column(const BraStage& st, const double* __r
                         X[hidx(t, u, w)] = pref * s;
                     }
             // bra step: v[(ka,kb),ab][kk] += C[ka,kb] f_ab sum_box E^{ab}_tuv X[tuv] ck[kk]
-            const double* E = st.E + (size_t)ib * BE::SIZE;
+            const RT* E = st.E + (size_t)ib * BE::SIZE;
 #pragma unroll UH
             for (int ia = 0; ia < Q::NA; ++ia) {
                 const int ax = cart_x(LA, ia), ay = cart_y(LA, ia), az = cart_z(LA, ia);
 #pragma unroll
                 for (int jb = 0; jb < Q::NB; ++jb) {
                     const int bx = cart_x(LB, jb), by = cart_y(LB, jb), bz = cart_z(LB, jb);
-                    const double fab = cart_norm(ax, ay, az) * cart_norm(bx, by, bz);
-                    double s = 0.0;
+                    const RT fab = static_cast<RT>(cart_norm(ax, ay, az) * cart_norm(bx, by, bz));
+                    RT s = RT(0);
 #pragma unroll
                     for (int t = 0; t <= ax + bx; ++t)
 #pragma unroll
                         for (int u = 0; u <= ay + by; ++u) {
-                            const double exy = E[BE::at(0, ax, bx, t)] * E[BE::at(1, ay, by, u)];
+                            const RT exy = E[BE::at(0, ax, bx, t)] * E[BE::at(1, ay, by, u)];
 #pragma unroll
                             for (int w = 0; w <= az + bz; ++w) s += exy * E[BE::at(2, az, bz, w)] * X[hidx(t, u, w)];
                         }
                     s *= fab;
 #pragma unroll
                     for (int kab = 0; kab < Q::KAB; ++kab) {
-                        const double c = sb[8 + kab] * s;
+                        const RT c = sb[8 + kab] * s;
 #pragma unroll
                         for (int kk = 0; kk < Q::KG; ++kk) v[kab * Q::NAB + ia * Q::NB + jb][kk] += c * ck[kk];
                     }
@@ -238,13 +239,35 @@ struct QuartetArgs {
     const int* sorted;          // [npair] pair index at sorted position
     const double* sortedQ;      // [npair]
     const int64_t* counts;      // [NSEG][npair + 1] kept ket prefix length per (ket segment, bra position)
+    // mixed precision: [NSEG][npair + 1] prefix with Q1 Q2 >= the FP32
+    // cutoff (evaluated in FP64); the rest of the kept prefix runs in FP32.
+    // nullptr: everything in FP64.
+    const int64_t* counts_hi;
     const int* seg_start;       // [NSEG + 1] sorted position of each segment (device)
     int npair;
     int cls_start[NCLS + 1];    // sorted positions of each angular class (geometry independent)
     int nao;
 };
 
-__device__ __forceinline__ void load_stage(const QuartetArgs& a, int P1, BraStage& st, double* E) {
+// Ket range [b, e) of segment seg for bra position spos that the kernels of
+// arithmetic type RT evaluate: the FP64 prefix, or the FP32 tail.
+template <typename RT>
+__device__ __forceinline__ void ket_range(const QuartetArgs& a, int seg, int spos, int64_t& b, int64_t& e) {
+    const size_t i = (size_t)seg * (a.npair + 1) + spos;
+    const int64_t cnt = a.counts[i];
+    int64_t hi = cnt;
+    if (a.counts_hi) hi = a.counts_hi[i] < cnt ? a.counts_hi[i] : cnt;
+    if constexpr (sizeof(RT) == sizeof(double)) {
+        b = 0;
+        e = hi;
+    } else {
+        b = hi;
+        e = a.counts_hi ? cnt : hi;
+    }
+}
+
+template <typename RT>
+__device__ __forceinline__ void load_stage(const QuartetArgs& a, int P1, BraStageT<RT>& st, RT* E) {
     st.P1 = P1;
     st.A = a.pv.pa_blk[P1];
     st.B = a.pv.pb_blk[P1];
@@ -281,8 +304,8 @@ struct JKArgs {
 // (m in A, n in B, l in C, s in D); the host forms J + J^T and K + K^T.
 // K rows m, n belong to the bra pair: Ksm[set][slot][col], slot < KA*NA for
 // A's functions, then B's.
-template <int CX, int CY, int NS, bool KGLOBAL>
-__device__ __forceinline__ void jk_digest_column(const JKArgs& a, const BraStage& st, int P2, int C, int Dd, int ic,
+template <int CX, int CY, int NS, bool KGLOBAL, typename ST>
+__device__ __forceinline__ void jk_digest_column(const JKArgs& a, const ST& st, int P2, int C, int Dd, int ic,
                                                  int id, int kg,
                                                  const double (&v)[QClass<CX, CY>::NROW][QClass<CX, CY>::KG],
                                                  double* Jt, double* Ksm) {
@@ -412,17 +435,18 @@ __device__ __forceinline__ void ket_items(int j0, int64_t cnt, KetQueue& q, int&
     }
 }
 
-template <int CX, int CY, int NS, bool KGLOBAL>
-__device__ __forceinline__ void jk_ket_class(const JKArgs& a, const BraStage& st, int spos, double* Jt, double* Ksm,
-                                             KetQueue& kq, int& rot) {
+template <int CX, int CY, int NS, bool KGLOBAL, typename RT>
+__device__ __forceinline__ void jk_ket_class(const JKArgs& a, const BraStageT<RT>& st, int spos, double* Jt,
+                                             double* Ksm, KetQueue& kq, int& rot) {
     using Q = QClass<CX, CY>;
     const double q1 = a.q.sortedQ[spos];
     const double* bm = a.bmax;
     const int nb = a.nblock;
     for (int sub = 0; sub < NSUB; ++sub) {
         const int seg = CY * NSUB + sub;
-        const int64_t cnt = a.q.counts[(size_t)seg * (a.q.npair + 1) + spos];
-        if (cnt == 0) continue;
+        int64_t kb, ke;
+        ket_range<RT>(a.q, seg, spos, kb, ke);
+        if (ke <= kb) continue;
         // difference densities: density-weighted test on the six block pairs
         auto keep = [&](int pos) {
             if (!bm) return true;
@@ -438,11 +462,21 @@ __device__ __forceinline__ void jk_ket_class(const JKArgs& a, const BraStage& st
             const int P2 = a.q.sorted[pos];
             const int C = a.q.pv.pa_blk[P2], Dd = a.q.pv.pb_blk[P2];
             const int ic = cd / Q::ND, id = cd % Q::ND;
-            double v[Q::NROW][Q::KG];
+            RT v[Q::NROW][Q::KG];
             eri_column<CX, CY>(st, a.q.pv.rec + a.q.pv.slot[P2] * PPW, a.q.pv.npp[P2], ic, id, kg, v);
-            jk_digest_column<CX, CY, NS, KGLOBAL>(a, st, P2, C, Dd, ic, id, kg, v, Jt, Ksm);
+            if constexpr (sizeof(RT) == sizeof(double)) {
+                jk_digest_column<CX, CY, NS, KGLOBAL>(a, st, P2, C, Dd, ic, id, kg, v, Jt, Ksm);
+            } else {
+                // FP32 quartets: digested (accumulated) in FP64
+                double vd[Q::NROW][Q::KG];
+#pragma unroll
+                for (int r = 0; r < Q::NROW; ++r)
+#pragma unroll
+                    for (int k = 0; k < Q::KG; ++k) vd[r][k] = static_cast<double>(v[r][k]);
+                jk_digest_column<CX, CY, NS, KGLOBAL>(a, st, P2, C, Dd, ic, id, kg, vd, Jt, Ksm);
+            }
         };
-        ket_items<Q::NCD * Q::NKG>(a.q.seg_start[seg], cnt, kq, rot, keep, work);
+        ket_items<Q::NCD * Q::NKG>(a.q.seg_start[seg] + static_cast<int>(kb), ke - kb, kq, rot, keep, work);
     }
 }
 
@@ -464,19 +498,24 @@ struct JKKernel {
 // J_ab slots [NS][NROW][blockDim], bra stage.
 constexpr int JK_THREADS = 128;
 
-template <int CX, int NS>
-__global__ void __launch_bounds__(JK_THREADS) jk_bra_kernel(JKArgs a) {
+// RT = double: the FP64 quartets; RT = float: the FP32 quartets of the
+// mixed-precision path (their J/K contributions still accumulate in FP64).
+#ifndef AIMD_JK_MINB
+#define AIMD_JK_MINB 1
+#endif
+template <int CX, int NS, typename RT>
+__global__ void __launch_bounds__(JK_THREADS, AIMD_JK_MINB) jk_bra_kernel(JKArgs a) {
     using KK = JKKernel<CX, NS>;
     using Q0 = QClass<CX, 0>;
     extern __shared__ double smem[];
     const int n = a.q.nao;
     double* Ksm = smem;
     double* Jt = Ksm + (size_t)KK::KROWS * n;
-    double* Esm = Jt + NS * KK::NROW * JK_THREADS;
+    RT* Esm = reinterpret_cast<RT*>(Jt + NS * KK::NROW * JK_THREADS);
     const int yk = KK::SPLIT ? (int)(blockIdx.x % KK::NY) : -1;
     const int spos = a.q.cls_start[CX] + (int)(blockIdx.x / KK::NY);
     const int P1 = a.q.sorted[spos];
-    __shared__ BraStage st;
+    __shared__ BraStageT<RT> st;
     __shared__ KetQueue kq;
     __shared__ int any;
     if (threadIdx.x == 0) {
@@ -484,7 +523,11 @@ __global__ void __launch_bounds__(JK_THREADS) jk_bra_kernel(JKArgs a) {
         int64_t tot = 0;
         for (int y = 0; y <= CX; ++y)
             if (yk < 0 || y == yk)
-                for (int sub = 0; sub < NSUB; ++sub) tot += a.q.counts[(size_t)(y * NSUB + sub) * (a.q.npair + 1) + spos];
+                for (int sub = 0; sub < NSUB; ++sub) {
+                    int64_t kb, ke;
+                    ket_range<RT>(a.q, y * NSUB + sub, spos, kb, ke);
+                    tot += ke > kb ? ke - kb : 0;
+                }
         any = tot > 0;
     }
     __syncthreads();
@@ -494,12 +537,12 @@ __global__ void __launch_bounds__(JK_THREADS) jk_bra_kernel(JKArgs a) {
     __syncthreads();
     constexpr bool KG_ = KK::KGLOBAL;
     int rot = 0;
-    if (yk < 0 || yk == 0) jk_ket_class<CX, 0, NS, KG_>(a, st, spos, Jt, Ksm, kq, rot);
-    if constexpr (CX >= 1) if (yk < 0 || yk == 1) jk_ket_class<CX, 1, NS, KG_>(a, st, spos, Jt, Ksm, kq, rot);
-    if constexpr (CX >= 2) if (yk < 0 || yk == 2) jk_ket_class<CX, 2, NS, KG_>(a, st, spos, Jt, Ksm, kq, rot);
-    if constexpr (CX >= 3) if (yk < 0 || yk == 3) jk_ket_class<CX, 3, NS, KG_>(a, st, spos, Jt, Ksm, kq, rot);
-    if constexpr (CX >= 4) if (yk < 0 || yk == 4) jk_ket_class<CX, 4, NS, KG_>(a, st, spos, Jt, Ksm, kq, rot);
-    if constexpr (CX >= 5) if (yk < 0 || yk == 5) jk_ket_class<CX, 5, NS, KG_>(a, st, spos, Jt, Ksm, kq, rot);
+    if (yk < 0 || yk == 0) jk_ket_class<CX, 0, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot);
+    if constexpr (CX >= 1) if (yk < 0 || yk == 1) jk_ket_class<CX, 1, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot);
+    if constexpr (CX >= 2) if (yk < 0 || yk == 2) jk_ket_class<CX, 2, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot);
+    if constexpr (CX >= 3) if (yk < 0 || yk == 3) jk_ket_class<CX, 3, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot);
+    if constexpr (CX >= 4) if (yk < 0 || yk == 4) jk_ket_class<CX, 4, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot);
+    if constexpr (CX >= 5) if (yk < 0 || yk == 5) jk_ket_class<CX, 5, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot);
     __syncthreads();
     const size_t nn = (size_t)n * n;
     // flush J_ab: one thread per (set, row) sums the per-thread slots
@@ -526,11 +569,11 @@ __global__ void __launch_bounds__(JK_THREADS) jk_bra_kernel(JKArgs a) {
     }
 }
 
-template <int CX, int NS>
+template <int CX, int NS, typename RT>
 size_t jk_smem_bytes(int nao, int max_bra_prims) {
     using KK = JKKernel<CX, NS>;
-    return sizeof(double) * ((size_t)KK::KROWS * nao + (size_t)NS * KK::NROW * JK_THREADS +
-                             (size_t)max_bra_prims * (KK::ESIZE + SBW));
+    return sizeof(double) * ((size_t)KK::KROWS * nao + (size_t)NS * KK::NROW * JK_THREADS) +
+           sizeof(RT) * (size_t)max_bra_prims * (KK::ESIZE + SBW);
 }
 
 // ---------------------------------------------------------- Schwarz

@@ -34,11 +34,11 @@ struct GradArgs {
 
 // For runtime (i, j): row[t] = E^{ij}_t and drow[t] = 2c E^{i+1,j}_t - i E^{i-1,j}_t
 // (the d/dC_x expansion), selected by predicated copies.
-template <int LC, int LD>
-__device__ __forceinline__ void ket_deriv_rows(const double (&e)[LC + 2][LD + 1][LC + LD + 2], int i, int j, double c,
-                                               double (&row)[LC + LD + 2], double (&drow)[LC + LD + 2]) {
+template <int LC, int LD, typename RT>
+__device__ __forceinline__ void ket_deriv_rows(const RT (&e)[LC + 2][LD + 1][LC + LD + 2], int i, int j, RT c,
+                                               RT (&row)[LC + LD + 2], RT (&drow)[LC + LD + 2]) {
 #pragma unroll
-    for (int t = 0; t <= LC + LD + 1; ++t) row[t] = drow[t] = 0.0;
+    for (int t = 0; t <= LC + LD + 1; ++t) row[t] = drow[t] = RT(0);
 #pragma unroll
     for (int ii = 0; ii <= LC; ++ii)
 #pragma unroll
@@ -46,15 +46,15 @@ __device__ __forceinline__ void ket_deriv_rows(const double (&e)[LC + 2][LD + 1]
             if (ii == i && jj == j)
 #pragma unroll
                 for (int t = 0; t <= LC + LD + 1; ++t) {
-                    row[t] = t <= LC + LD ? e[ii][jj][t] : 0.0;
-                    drow[t] = 2.0 * c * e[ii + 1][jj][t] - (ii > 0 ? ii * e[ii > 0 ? ii - 1 : 0][jj][t] : 0.0);
+                    row[t] = t <= LC + LD ? e[ii][jj][t] : RT(0);
+                    drow[t] = RT(2) * c * e[ii + 1][jj][t] - (ii > 0 ? ii * e[ii > 0 ? ii - 1 : 0][jj][t] : RT(0));
                 }
 }
 
 // Gradient contribution of one column; adds A, B parts to gab and C, D
 // parts to the shared accumulator gsh[natm][3].
-template <int CX, int CY>
-__device__ __forceinline__ void grad_column(const GradArgs& a, const BraStage& st, int P2, double QQ, int ic,
+template <int CX, int CY, typename RT>
+__device__ __forceinline__ void grad_column(const GradArgs& a, const BraStageT<RT>& st, int P2, double QQ, int ic,
                                             int id, int kg, double (&gab)[6], double* gsh) {
     using Q = QClass<CX, CY>;
     using BE = BraE<Q::LA, Q::LB, 1>;
@@ -97,78 +97,84 @@ __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStage& s
         }
     }
     if (QQ == 0.0 || QQ * gmax < a.thr) return;
-    double dA[3] = {0.0, 0.0, 0.0}, dB[3] = {0.0, 0.0, 0.0}, dC[3] = {0.0, 0.0, 0.0};
+    // the Gamma column in the arithmetic type of the quartet
+    RT Gr[Q::NROW][Q::KG];
+#pragma unroll
+    for (int r = 0; r < Q::NROW; ++r)
+#pragma unroll
+        for (int kk = 0; kk < Q::KG; ++kk) Gr[r][kk] = static_cast<RT>(G[r][kk]);
+    RT dA[3] = {0.0, 0.0, 0.0}, dB[3] = {0.0, 0.0, 0.0}, dC[3] = {0.0, 0.0, 0.0};
     const int cx = cart_x(LC, ic), cy = cart_y(LC, ic), cz = cart_z(LC, ic);
     const int dx = cart_x(LD, id), dy = cart_y(LD, id), dz = cart_z(LD, id);
-    const double fcd = cart_norm(cx, cy, cz) * cart_norm(dx, dy, dz);
+    const RT fcd = cart_norm(cx, cy, cz) * cart_norm(dx, dy, dz);
     const double* rk = a.q.pv.rec + a.q.pv.slot[P2] * PPW;
     const int nkp = a.q.pv.npp[P2];
     for (int ik = 0; ik < nkp; ++ik) {
-        const KetRec k = load_ket(rk + (size_t)ik * PPW);
-        const double ec = k.a, q = ec + k.b, oo2q = 0.5 / q, iq = 2.0 * oo2q;
+        const KetRecT<RT> k = load_ket<RT>(rk + (size_t)ik * PPW);
+        const RT ec = k.a, q = ec + k.b, oo2q = RT(0.5) / q, iq = RT(2) * oo2q;
         // ket E for this column, and d/dC_d of it (one extra in direction d)
-        double ex[LCD + 2], ey[LCD + 2], ez[LCD + 2], gx[LCD + 2], gy[LCD + 2], gz[LCD + 2];
+        RT ex[LCD + 2], ey[LCD + 2], ez[LCD + 2], gx[LCD + 2], gy[LCD + 2], gz[LCD + 2];
         {
-            double e[LC + 2][LD + 1][LCD + 2];
+            RT e[LC + 2][LD + 1][LCD + 2];
             hermite_e<LC + 1, LD>(k.QAx, k.QBx, oo2q, k.K, e);
             ket_deriv_rows<LC, LD>(e, cx, dx, ec, ex, gx);
-            hermite_e<LC + 1, LD>(k.QAy, k.QBy, oo2q, 1.0, e);
+            hermite_e<LC + 1, LD>(k.QAy, k.QBy, oo2q, RT(1), e);
             ket_deriv_rows<LC, LD>(e, cy, dy, ec, ey, gy);
-            hermite_e<LC + 1, LD>(k.QAz, k.QBz, oo2q, 1.0, e);
+            hermite_e<LC + 1, LD>(k.QAz, k.QBz, oo2q, RT(1), e);
             ket_deriv_rows<LC, LD>(e, cz, dz, ec, ez, gz);
         }
-        double ck[Q::KG];
+        RT ck[Q::KG];
 #pragma unroll
         for (int i = 0; i < Q::KG; ++i) {
-            double c = k.c[0];
+            RT c = k.c[0];
 #pragma unroll
             for (int j = 1; j < Q::KCD; ++j)
                 if (j == kg * Q::KG + i) c = k.c[j];
             ck[i] = c * fcd;
         }
         for (int ib = 0; ib < st.nbp; ++ib) {
-            const double* sb = st.SB + ib * SBW;
-            const double p = sb[0], ea = sb[5], eb = sb[6];
-            const double rs = rsqrt(p + q);
-            const double alpha = p * q * rs * rs;
-            const double pref = TWO_PI_2_5 * sb[1] * iq * rs;
-            const double* E = st.E + (size_t)ib * BE::SIZE;
-            double R[nherm(L)];
+            const RT* sb = st.SB + ib * SBW;
+            const RT p = sb[0], ea = sb[5], eb = sb[6];
+            const RT rs = rsqrt_t(p + q);
+            const RT alpha = p * q * rs * rs;
+            const RT pref = RT(TWO_PI_2_5) * sb[1] * iq * rs;
+            const RT* E = st.E + (size_t)ib * BE::SIZE;
+            RT R[nherm(L)];
             hermite_r<L>(alpha, sb[2] - k.Qx, sb[3] - k.Qy, sb[4] - k.Qz, R);
             // Gamma contracted with this bra primitive's coefficients and f_ab,
             // then summed over the ket contractions: gq[ab] = sum_kk gb[ab][kk] ck[kk]
-            double gq[Q::NAB];
+            RT gq[Q::NAB];
 #pragma unroll
             for (int ia = 0; ia < Q::NA; ++ia)
 #pragma unroll
                 for (int jb = 0; jb < Q::NB; ++jb) {
-                    const double fab = cart_norm(cart_x(LA, ia), cart_y(LA, ia), cart_z(LA, ia)) *
+                    const RT fab = cart_norm(cart_x(LA, ia), cart_y(LA, ia), cart_z(LA, ia)) *
                                        cart_norm(cart_x(LB, jb), cart_y(LB, jb), cart_z(LB, jb));
                     const int ab = ia * Q::NB + jb;
-                    double s = 0.0;
+                    RT s = 0.0;
 #pragma unroll
                     for (int kab = 0; kab < Q::KAB; ++kab)
 #pragma unroll
-                        for (int kk = 0; kk < Q::KG; ++kk) s += sb[8 + kab] * G[kab * Q::NAB + ab][kk] * ck[kk];
+                        for (int kk = 0; kk < Q::KG; ++kk) s += sb[8 + kab] * Gr[kab * Q::NAB + ab][kk] * ck[kk];
                     gq[ab] = s * fab * pref;
                 }
             // bra pass (A, B): sum_ab gq[ab] sum_{h in dbox(ab)} dE_h Xb_h,
             // Xb_h = sum_{k in box(cd)} (-1)^|k| E^{cd}_k R_{h+k}
-            double Xb[NH1];
+            RT Xb[NH1];
 #pragma unroll UH
             for (int t = 0; t <= LAB + 1; ++t)
 #pragma unroll UH
                 for (int u = 0; u <= LAB + 1 - t; ++u)
 #pragma unroll UW
                     for (int w = 0; w <= LAB + 1 - t - u; ++w) {
-                        double s = 0.0;
+                        RT s = 0.0;
 #pragma unroll
                         for (int t2 = 0; t2 <= LCD; ++t2) {
                             if (t2 > cx + dx) continue;
 #pragma unroll
                             for (int u2 = 0; u2 <= LCD; ++u2) {
                                 if (u2 > cy + dy) continue;
-                                const double exy = ((t2 + u2) & 1) ? -ex[t2] * ey[u2] : ex[t2] * ey[u2];
+                                const RT exy = ((t2 + u2) & 1) ? -ex[t2] * ey[u2] : ex[t2] * ey[u2];
 #pragma unroll
                                 for (int v2 = 0; v2 <= LCD; ++v2) {
                                     if (v2 > cz + dz) continue;
@@ -180,7 +186,7 @@ __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStage& s
                     }
             // C pass: Y_h = sum_ab gq[ab] E^{ab}_h (h <= LAB), then
             // dC_d += sum_h Y_h sum_k (-1)^|k| dE^{cd}_{d,k} R_{h+k}
-            double Y[Q::NHB];
+            RT Y[Q::NHB];
 #pragma unroll
             for (int h = 0; h < Q::NHB; ++h) Y[h] = 0.0;
 #pragma unroll UH
@@ -189,7 +195,7 @@ __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStage& s
 #pragma unroll
                 for (int jb = 0; jb < Q::NB; ++jb) {
                     const int bx = cart_x(LB, jb), by = cart_y(LB, jb), bz = cart_z(LB, jb);
-                    const double g = gq[ia * Q::NB + jb];
+                    const RT g = gq[ia * Q::NB + jb];
 #pragma unroll
                     for (int t = 0; t <= ax + bx + 1; ++t)
 #pragma unroll
@@ -198,16 +204,16 @@ __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStage& s
                             for (int w = 0; w <= az + bz + 1; ++w) {
                                 const int over = (t > ax + bx) + (u > ay + by) + (w > az + bz);
                                 if (over > 1) continue;
-                                const double yv = g * Xb[hidx(t, u, w)];
-                                const double e0 = E[BE::at(0, ax, bx, t)], e1 = E[BE::at(1, ay, by, u)],
+                                const RT yv = g * Xb[hidx(t, u, w)];
+                                const RT e0 = E[BE::at(0, ax, bx, t)], e1 = E[BE::at(1, ay, by, u)],
                                              e2 = E[BE::at(2, az, bz, w)];
                                 if (over == 0) Y[hidx(t, u, w)] += g * e0 * e1 * e2;
-                                const double dax = 2.0 * ea * E[BE::at(0, ax + 1, bx, t)] - (ax > 0 ? ax * E[BE::at(0, ax > 0 ? ax - 1 : 0, bx, t)] : 0.0);
-                                const double day = 2.0 * ea * E[BE::at(1, ay + 1, by, u)] - (ay > 0 ? ay * E[BE::at(1, ay > 0 ? ay - 1 : 0, by, u)] : 0.0);
-                                const double daz = 2.0 * ea * E[BE::at(2, az + 1, bz, w)] - (az > 0 ? az * E[BE::at(2, az > 0 ? az - 1 : 0, bz, w)] : 0.0);
-                                const double dbx = 2.0 * eb * E[BE::at(0, ax, bx + 1, t)] - (bx > 0 ? bx * E[BE::at(0, ax, bx > 0 ? bx - 1 : 0, t)] : 0.0);
-                                const double dby = 2.0 * eb * E[BE::at(1, ay, by + 1, u)] - (by > 0 ? by * E[BE::at(1, ay, by > 0 ? by - 1 : 0, u)] : 0.0);
-                                const double dbz = 2.0 * eb * E[BE::at(2, az, bz + 1, w)] - (bz > 0 ? bz * E[BE::at(2, az, bz > 0 ? bz - 1 : 0, w)] : 0.0);
+                                const RT dax = RT(2) * ea * E[BE::at(0, ax + 1, bx, t)] - (ax > 0 ? ax * E[BE::at(0, ax > 0 ? ax - 1 : 0, bx, t)] : RT(0));
+                                const RT day = RT(2) * ea * E[BE::at(1, ay + 1, by, u)] - (ay > 0 ? ay * E[BE::at(1, ay > 0 ? ay - 1 : 0, by, u)] : RT(0));
+                                const RT daz = RT(2) * ea * E[BE::at(2, az + 1, bz, w)] - (az > 0 ? az * E[BE::at(2, az > 0 ? az - 1 : 0, bz, w)] : RT(0));
+                                const RT dbx = RT(2) * eb * E[BE::at(0, ax, bx + 1, t)] - (bx > 0 ? bx * E[BE::at(0, ax, bx > 0 ? bx - 1 : 0, t)] : RT(0));
+                                const RT dby = RT(2) * eb * E[BE::at(1, ay, by + 1, u)] - (by > 0 ? by * E[BE::at(1, ay, by > 0 ? by - 1 : 0, u)] : RT(0));
+                                const RT dbz = RT(2) * eb * E[BE::at(2, az, bz + 1, w)] - (bz > 0 ? bz * E[BE::at(2, az, bz > 0 ? bz - 1 : 0, w)] : RT(0));
                                 dA[0] += yv * dax * e1 * e2;
                                 dA[1] += yv * e0 * day * e2;
                                 dA[2] += yv * e0 * e1 * daz;
@@ -223,8 +229,8 @@ __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStage& s
                 for (int u = 0; u <= LAB - t; ++u)
 #pragma unroll UW
                     for (int w = 0; w <= LAB - t - u; ++w) {
-                        const double yv = Y[hidx(t, u, w)];
-                        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+                        const RT yv = Y[hidx(t, u, w)];
+                        RT s0 = 0.0, s1 = 0.0, s2 = 0.0;
 #pragma unroll
                         for (int t2 = 0; t2 <= LCD + 1; ++t2) {
                             if (t2 > cx + dx + 1) continue;
@@ -236,7 +242,7 @@ __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStage& s
                                     if (v2 > cz + dz + 1) continue;
                                     const int over = (t2 > cx + dx) + (u2 > cy + dy) + (v2 > cz + dz);
                                     if (over > 1) continue;
-                                    const double r = ((t2 + u2 + v2) & 1) ? -R[hidx(t + t2, u + u2, w + v2)]
+                                    const RT r = ((t2 + u2 + v2) & 1) ? -R[hidx(t + t2, u + u2, w + v2)]
                                                                           : R[hidx(t + t2, u + u2, w + v2)];
                                     s0 += gx[t2] * ey[u2] * ez[v2] * r;
                                     s1 += ex[t2] * gy[u2] * ez[v2] * r;
@@ -252,10 +258,11 @@ __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStage& s
     }
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        gab[d] += dA[d];
-        gab[3 + d] += dB[d];
-        atomicAdd(gsh + 3 * aC + d, dC[d]);
-        atomicAdd(gsh + 3 * aD + d, -(dA[d] + dB[d] + dC[d]));
+        const double da = dA[d], db = dB[d], dc = dC[d];
+        gab[d] += da;
+        gab[3 + d] += db;
+        atomicAdd(gsh + 3 * aC + d, dc);
+        atomicAdd(gsh + 3 * aD + d, -(da + db + dc));
     }
 }
 
@@ -263,8 +270,8 @@ __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStage& s
 // block quartet, deg [|Dc|_AB |Dc|_CD + |k|/2 nx (|Dx|_AC |Dx|_BD +
 // |Dx|_AD |Dx|_BC)] >= max|Gamma|, can reach the threshold and the quartet
 // is not one-centre; the exact per-column test follows in grad_column.
-template <int CX, int CY>
-__device__ __forceinline__ void grad_ket_class(const GradArgs& a, const BraStage& st, int spos, double (&gab)[6],
+template <int CX, int CY, typename RT>
+__device__ __forceinline__ void grad_ket_class(const GradArgs& a, const BraStageT<RT>& st, int spos, double (&gab)[6],
                                                double* gsh, KetQueue& kq, int& rot) {
     using Q = QClass<CX, CY>;
     const double q1 = a.q.sortedQ[spos];
@@ -272,8 +279,9 @@ __device__ __forceinline__ void grad_ket_class(const GradArgs& a, const BraStage
     const double xf = 0.5 * fabs(a.kfac) * a.nx;
     for (int sub = 0; sub < NSUB; ++sub) {
         const int seg = CY * NSUB + sub;
-        const int64_t cnt = a.q.counts[(size_t)seg * (a.q.npair + 1) + spos];
-        if (cnt == 0) continue;
+        int64_t kb, ke;
+        ket_range<RT>(a.q, seg, spos, kb, ke);
+        if (ke <= kb) continue;
         auto keep = [&](int pos) {
             const int P2 = a.q.sorted[pos];
             const int C = a.q.pv.pa_blk[P2], Dd = a.q.pv.pb_blk[P2];
@@ -287,29 +295,39 @@ __device__ __forceinline__ void grad_ket_class(const GradArgs& a, const BraStage
         };
         auto work = [&](int pos, int r) {
             const int kg = r % Q::NKG, cd = r / Q::NKG;
-            grad_column<CX, CY>(a, st, a.q.sorted[pos], q1 * a.q.sortedQ[pos], cd / Q::ND, cd % Q::ND, kg, gab, gsh);
+            grad_column<CX, CY, RT>(a, st, a.q.sorted[pos], q1 * a.q.sortedQ[pos], cd / Q::ND, cd % Q::ND, kg, gab,
+                                    gsh);
         };
-        ket_items<Q::NCD * Q::NKG>(a.q.seg_start[seg], cnt, kq, rot, keep, work);
+        ket_items<Q::NCD * Q::NKG>(a.q.seg_start[seg] + static_cast<int>(kb), ke - kb, kq, rot, keep, work);
     }
 }
 
 // One kernel per (bra class, ket class): CTA per bra pair of class CX, items
 // over the ket segments of class CY. Dynamic shared memory: gradient
 // accumulator [natm][3], bra E tables (+1).
-template <int CX, int CY>
-__global__ void __launch_bounds__(128) grad2e_bra_kernel(GradArgs a) {
+// RT = double: the FP64 quartets; RT = float: the FP32 quartets of the
+// mixed-precision path (accumulated in FP64).
+#ifndef AIMD_GRAD_MINB
+#define AIMD_GRAD_MINB 1
+#endif
+template <int CX, int CY, typename RT>
+__global__ void __launch_bounds__(128, AIMD_GRAD_MINB) grad2e_bra_kernel(GradArgs a) {
     using Q0 = QClass<CX, 0>;
     extern __shared__ double smem[];
     double* gsh = smem;
-    double* Esm = smem + 3 * a.natm;
-    __shared__ BraStage st;
+    RT* Esm = reinterpret_cast<RT*>(smem + 3 * a.natm);
+    __shared__ BraStageT<RT> st;
     __shared__ KetQueue kq;
     __shared__ int any;
     const int spos = a.q.cls_start[CX] + blockIdx.x;
     if (threadIdx.x == 0) {
         load_stage(a.q, a.q.sorted[spos], st, Esm);
         int64_t tot = 0;
-        for (int sub = 0; sub < NSUB; ++sub) tot += a.q.counts[(size_t)(CY * NSUB + sub) * (a.q.npair + 1) + spos];
+        for (int sub = 0; sub < NSUB; ++sub) {
+            int64_t kb, ke;
+            ket_range<RT>(a.q, CY * NSUB + sub, spos, kb, ke);
+            tot += ke > kb ? ke - kb : 0;
+        }
         any = tot > 0;
     }
     __syncthreads();
@@ -319,7 +337,7 @@ __global__ void __launch_bounds__(128) grad2e_bra_kernel(GradArgs a) {
     __syncthreads();
     double gab[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     int rot = 0;
-    grad_ket_class<CX, CY>(a, st, spos, gab, gsh, kq, rot);
+    grad_ket_class<CX, CY, RT>(a, st, spos, gab, gsh, kq, rot);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         if (gab[d] != 0.0) atomicAdd(gsh + 3 * st.aA + d, gab[d]);
@@ -330,10 +348,10 @@ __global__ void __launch_bounds__(128) grad2e_bra_kernel(GradArgs a) {
         if (gsh[i] != 0.0) atomicAdd(a.grad + i, gsh[i]);
 }
 
-template <int CX>
+template <int CX, typename RT>
 size_t grad_smem_bytes(int natm, int max_bra_prims) {
     using Q0 = QClass<CX, 0>;
-    return sizeof(double) * (3 * (size_t)natm + (size_t)max_bra_prims * (BraE<Q0::LA, Q0::LB, 1>::SIZE + SBW));
+    return sizeof(double) * 3 * (size_t)natm + sizeof(RT) * (size_t)max_bra_prims * (BraE<Q0::LA, Q0::LB, 1>::SIZE + SBW);
 }
 
 }  // namespace hf

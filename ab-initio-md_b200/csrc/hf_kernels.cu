@@ -76,6 +76,10 @@ struct aimd_ctx {
     cudaEvent_t ev_fork, ev_join[NCLS];
     int maxbp[NCLS];        // largest primitive-pair count of a block pair, per class
     double thr_jk = -1.0, thr_g = -1.0;
+    // mixed precision: quartets with Q1 Q2 < fp32_cutoff run in FP32
+    // (0: all FP64); counts_hi is the FP64 prefix table, built at thr_hi
+    double fp32_cutoff = 0.0, thr_hi = -1.0;
+    int64_t* counts_hi;
     void* cub_tmp;
     size_t cub_bytes;
     double* pos;            // [natm][3] device copy of the current geometry
@@ -210,6 +214,7 @@ extern "C" int aimd_create(aimd_ctx** out, int natm, int nao, int nblock, const 
         CK(dalloc(&c->counts_jk, (size_t)NSEG * (np + 1)));
         CK(dalloc(&c->counts_g, (size_t)NSEG * (np + 1)));
         CK(dalloc(&c->counts_d, (size_t)NSEG * (np + 1)));
+        CK(dalloc(&c->counts_hi, (size_t)NSEG * (np + 1)));
         CK(dalloc(&c->bmax, (size_t)nblock * nblock));
         CK(dalloc(&c->dmax, 1));
         CK(dalloc(&c->bmc, (size_t)nblock * nblock));
@@ -238,7 +243,7 @@ extern "C" int aimd_destroy(aimd_ctx* c) {
                     c->sh_atom, c->sh_l, c->sh_ao, c->sh_p0, c->sh_np, c->sp_i, c->sp_j, c->sh_exp, c->sh_coef,
                     c->charges, c->pa, c->pb, c->npp, c->slot, c->rec, c->Q, c->by_class, c->idx_in,
                     c->tmp_idx, c->seg_id, c->seg_keys, c->seg_keys_out, c->seg_start, c->tmpQ, c->sortedQ,
-                    c->sorted, c->counts_jk, c->counts_g, c->counts_d, c->bmax, c->dmax, c->bmc, c->bmx, c->cub_tmp, c->pos};
+                    c->sorted, c->counts_jk, c->counts_g, c->counts_d, c->bmax, c->dmax, c->bmc, c->bmx, c->counts_hi, c->cub_tmp, c->pos};
     for (void* p : ptrs) cudaFree(p);
     for (int i = 0; i < NCLS; ++i) {
         if (c->cls_stream[i]) cudaStreamDestroy(c->cls_stream[i]);
@@ -406,6 +411,7 @@ QuartetArgs quartet_args(aimd_ctx* c, const int64_t* counts) {
     q.sorted = c->sorted;
     q.sortedQ = c->sortedQ;
     q.counts = counts;
+    q.counts_hi = nullptr;
     q.seg_start = c->seg_start;
     q.npair = c->npair;
     for (int i = 0; i <= NCLS; ++i) q.cls_start[i] = c->cls_start[i];
@@ -445,8 +451,10 @@ LaunchEnv launch_env(aimd_ctx* c) {
 template <int CX>
 cudaError_t launch_grad_class(const LaunchEnv& e, const GradArgs& a, cudaStream_t st) {
     cudaError_t r = cudaSuccess;
-#define AIMD_G1(X, Y) \
-    if (r == cudaSuccess && CX == X) r = launch_grad_c##X##_##Y(e, a, st);
+    const bool mixed = a.q.counts_hi != nullptr;
+#define AIMD_G1(X, Y)                                                             \
+    if (r == cudaSuccess && CX == X) r = launch_grad_c##X##_##Y(e, a, st);       \
+    if (r == cudaSuccess && CX == X && mixed) r = launch_grad32_c##X##_##Y(e, a, st);
     AIMD_G1(0, 0)
     AIMD_G1(1, 0) AIMD_G1(1, 1)
     AIMD_G1(2, 0) AIMD_G1(2, 1) AIMD_G1(2, 2)
@@ -457,9 +465,21 @@ cudaError_t launch_grad_class(const LaunchEnv& e, const GradArgs& a, cudaStream_
     return r;
 }
 
-int class_status(aimd_ctx* c, cudaError_t r, const char* what, int cl) {
+// kernel launches of one class step: J/K one per type, the gradient one
+// per (bra class, non-empty ket class) and type
+int cls_size(aimd_ctx* c, int cl) { return c->cls_start[cl + 1] - c->cls_start[cl]; }
+int jk_launches(aimd_ctx* c, int cl, bool mixed) { return cls_size(c, cl) > 0 ? (mixed ? 2 : 1) : 0; }
+int grad_launches(aimd_ctx* c, int cl, bool mixed) {
+    int n = 0;
+    for (int y = 0; y <= cl; ++y) n += (cls_size(c, cl) > 0 && cls_size(c, y) > 0) ? 1 : 0;
+    return mixed ? 2 * n : n;
+}
+
+inline cudaError_t first_error(cudaError_t a, cudaError_t b) { return a != cudaSuccess ? a : b; }
+
+int class_status(aimd_ctx* c, cudaError_t r, const char* what, int cl, int nlaunch) {
     if (r == cudaSuccess) {
-        if (c->cls_start[cl + 1] > c->cls_start[cl]) ++c->launches;
+        c->launches += nlaunch;
         return AIMD_OK;
     }
     if (r == cudaErrorInvalidConfiguration) {
@@ -474,18 +494,18 @@ int class_status(aimd_ctx* c, cudaError_t r, const char* what, int cl) {
 #define AIMD_EACH_CLASS(CALL, WHAT)                                         \
     do {                                                                    \
         int r_;                                                             \
-        if ((r_ = class_status(c, CALL(0), WHAT, 0))) return r_;            \
-        if ((r_ = class_status(c, CALL(1), WHAT, 1))) return r_;            \
-        if ((r_ = class_status(c, CALL(2), WHAT, 2))) return r_;            \
-        if ((r_ = class_status(c, CALL(3), WHAT, 3))) return r_;            \
-        if ((r_ = class_status(c, CALL(4), WHAT, 4))) return r_;            \
-        if ((r_ = class_status(c, CALL(5), WHAT, 5))) return r_;            \
+        if ((r_ = class_status(c, CALL(0), WHAT, 0, cls_size(c, 0) > 0))) return r_;  \
+        if ((r_ = class_status(c, CALL(1), WHAT, 1, cls_size(c, 1) > 0))) return r_;  \
+        if ((r_ = class_status(c, CALL(2), WHAT, 2, cls_size(c, 2) > 0))) return r_;  \
+        if ((r_ = class_status(c, CALL(3), WHAT, 3, cls_size(c, 3) > 0))) return r_;  \
+        if ((r_ = class_status(c, CALL(4), WHAT, 4, cls_size(c, 4) > 0))) return r_;  \
+        if ((r_ = class_status(c, CALL(5), WHAT, 5, cls_size(c, 5) > 0))) return r_;  \
     } while (0)
 
 // The six class launches of one call run concurrently on the context's
 // class streams, forked from and joined back into the caller's stream, so
 // the long-running d-shell classes overlap the others.
-#define AIMD_EACH_CLASS_CONCURRENT(CALL, WHAT)                                        \
+#define AIMD_EACH_CLASS_CONCURRENT(CALL, WHAT, NLAUNCH)                               \
     do {                                                                              \
         CK(cudaEventRecord(c->ev_fork, st));                                          \
         int r_ = AIMD_OK;                                                             \
@@ -501,14 +521,35 @@ int class_status(aimd_ctx* c, cudaError_t r, const char* what, int cl) {
                 case 4: e_ = CALL(4, cs_); break;                                     \
                 default: e_ = CALL(5, cs_); break;                                    \
             }                                                                         \
-            r_ = class_status(c, e_, WHAT, x_);                                       \
+            r_ = class_status(c, e_, WHAT, x_, NLAUNCH(x_));                          \
             CK(cudaEventRecord(c->ev_join[x_], cs_));                                 \
             CK(cudaStreamWaitEvent(st, c->ev_join[x_], 0));                           \
         }                                                                             \
         if (r_) return r_;                                                            \
     } while (0)
 
+// The FP64-prefix table of the mixed-precision path (nullptr when off).
+int hi_counts(aimd_ctx* c, cudaStream_t st, const int64_t** out) {
+    *out = nullptr;
+    if (!(c->fp32_cutoff > 0.0)) return AIMD_OK;
+    if (c->thr_hi != c->fp32_cutoff) {
+        if (int r = build_counts(c, c->fp32_cutoff, c->counts_hi, st)) return r;
+        c->thr_hi = c->fp32_cutoff;
+    }
+    *out = c->counts_hi;
+    return AIMD_OK;
+}
+
 }  // namespace
+
+extern "C" int aimd_set_fp32_cutoff(aimd_ctx* c, double cutoff) {
+    if (!c || !(cutoff >= 0.0) || !std::isfinite(cutoff)) {
+        snprintf(g_err, sizeof g_err, "aimd_set_fp32_cutoff: cutoff must be finite and >= 0");
+        return AIMD_ERR_ARG;
+    }
+    c->fp32_cutoff = cutoff;
+    return AIMD_OK;
+}
 
 extern "C" int aimd_set_geometry(aimd_ctx* c, const double* pos, void* stream) {
     if (!c || !pos) return AIMD_ERR_ARG;
@@ -540,7 +581,7 @@ extern "C" int aimd_set_geometry(aimd_ctx* c, const double* pos, void* stream) {
     seg_start_kernel<<<1, NSEG + 1, 0, st>>>(np, c->seg_keys_out, c->seg_start);
     c->launches += 6;
     CK(cudaGetLastError());
-    c->thr_jk = c->thr_g = -1.0;
+    c->thr_jk = c->thr_g = c->thr_hi = -1.0;
     c->have_geometry = true;
     return AIMD_OK;
 }
@@ -560,6 +601,9 @@ extern "C" int aimd_jk(aimd_ctx* c, int nset, const double* D, double* J, double
         if (int r = build_counts(c, thr, c->counts_jk, st)) return r;
         c->thr_jk = thr;
     }
+    const int64_t* hi = nullptr;
+    if (int r = hi_counts(c, st, &hi)) return r;
+    const bool mixed = hi != nullptr;
     const size_t nn = (size_t)c->nao * c->nao;
     CK(cudaMemsetAsync(J, 0, sizeof(double) * nset * nn, st));
     CK(cudaMemsetAsync(K, 0, sizeof(double) * nset * nn, st));
@@ -568,14 +612,17 @@ extern "C" int aimd_jk(aimd_ctx* c, int nset, const double* D, double* J, double
     for (int s0 = 0; s0 < nset; ++s0) {
         JKArgs a;
         a.q = quartet_args(c, c->counts_jk);
+        a.q.counts_hi = hi;
         a.D = D + s0 * nn;
         a.J = J + s0 * nn;
         a.K = K + s0 * nn;
         a.bmax = nullptr;
         a.nblock = c->nblock;
         a.dthr = 0.0;
-#define AIMD_JK(X, S) launch_jk_c##X(e, a, S)
-        AIMD_EACH_CLASS_CONCURRENT(AIMD_JK, "aimd_jk");
+#define AIMD_JK(X, S) first_error(launch_jk_c##X(e, a, S), mixed ? launch_jk32_c##X(e, a, S) : cudaSuccess)
+#define AIMD_NL(X) jk_launches(c, X, mixed)
+        AIMD_EACH_CLASS_CONCURRENT(AIMD_JK, "aimd_jk", AIMD_NL);
+#undef AIMD_NL
 #undef AIMD_JK
     }
     return AIMD_OK;
@@ -617,20 +664,26 @@ extern "C" int aimd_jk_delta(aimd_ctx* c, int nset, const double* D, double* J, 
     // enumerate at max(thr, dthr / max|D|): the integral screen still holds,
     // and no quartet that the density-weighted test keeps is missed
     if (int r = build_counts(c, dthr, c->counts_d, st, c->dmax, thr)) return r;
+    const int64_t* hi = nullptr;
+    if (int r = hi_counts(c, st, &hi)) return r;
+    const bool mixed = hi != nullptr;
     CK(cudaMemsetAsync(J, 0, sizeof(double) * nset * nn, st));
     CK(cudaMemsetAsync(K, 0, sizeof(double) * nset * nn, st));
     const LaunchEnv e = launch_env(c);
     for (int s0 = 0; s0 < nset; ++s0) {
         JKArgs a;
         a.q = quartet_args(c, c->counts_d);
+        a.q.counts_hi = hi;
         a.D = D + s0 * nn;
         a.J = J + s0 * nn;
         a.K = K + s0 * nn;
         a.bmax = c->bmax;
         a.nblock = c->nblock;
         a.dthr = dthr;
-#define AIMD_JK(X, S) launch_jk_c##X(e, a, S)
-        AIMD_EACH_CLASS_CONCURRENT(AIMD_JK, "aimd_jk_delta");
+#define AIMD_JK(X, S) first_error(launch_jk_c##X(e, a, S), mixed ? launch_jk32_c##X(e, a, S) : cudaSuccess)
+#define AIMD_NL(X) jk_launches(c, X, mixed)
+        AIMD_EACH_CLASS_CONCURRENT(AIMD_JK, "aimd_jk_delta", AIMD_NL);
+#undef AIMD_NL
 #undef AIMD_JK
     }
     return AIMD_OK;
@@ -762,8 +815,12 @@ extern "C" int aimd_grad2e(aimd_ctx* c, const double* Dc, int nx, const double* 
         ++c->launches;
     }
     CK(cudaGetLastError());
+    const int64_t* hi = nullptr;
+    if (int r = hi_counts(c, st, &hi)) return r;
+    const bool mixed = hi != nullptr;
     GradArgs a;
     a.q = quartet_args(c, c->counts_g);
+    a.q.counts_hi = hi;
     a.Dc = Dc;
     a.Dx = Dx;
     a.nx = nx;
@@ -776,7 +833,9 @@ extern "C" int aimd_grad2e(aimd_ctx* c, const double* Dc, int nx, const double* 
     a.nblock = c->nblock;
     const LaunchEnv e = launch_env(c);
 #define AIMD_GRAD(X, S) launch_grad_class<X>(e, a, S)
-    AIMD_EACH_CLASS_CONCURRENT(AIMD_GRAD, "aimd_grad2e");
+#define AIMD_NL(X) grad_launches(c, X, mixed)
+    AIMD_EACH_CLASS_CONCURRENT(AIMD_GRAD, "aimd_grad2e", AIMD_NL);
+#undef AIMD_NL
 #undef AIMD_GRAD
     return AIMD_OK;
 }

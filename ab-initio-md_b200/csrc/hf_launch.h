@@ -1,8 +1,10 @@
 // Host-side launchers of the class-templated kernels. Each bra pair class
 // lives in its own translation units (hf_class_jk.cu compiled with
 // -DAIMD_CLASS=0..5, hf_class_grad.cu with -DAIMD_CLASS=X -DAIMD_KET=Y for
-// Y <= X) so that they compile in parallel. Gradient launchers with Y > X
-// are declared but never defined or called.
+// Y <= X), once per arithmetic type (-DAIMD_REAL=0: FP64, the launchers
+// below without a suffix; -DAIMD_REAL=1: the FP32 quartets of the
+// mixed-precision path, suffix 32), so that they compile in parallel.
+// Gradient launchers with Y > X are declared but never defined or called.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -22,15 +24,18 @@ struct LaunchEnv {
 
 // Status: cudaSuccess, a CUDA error, or cudaErrorInvalidConfiguration when
 // the shared-memory request exceeds the per-CTA limit.
+#define AIMD_DECLARE_TYPED(X, S)                                                                       \
+    cudaError_t launch_jk##S##_c##X(const LaunchEnv& e, const JKArgs& a, cudaStream_t st);              \
+    cudaError_t launch_grad##S##_c##X##_0(const LaunchEnv& e, const GradArgs& a, cudaStream_t st);     \
+    cudaError_t launch_grad##S##_c##X##_1(const LaunchEnv& e, const GradArgs& a, cudaStream_t st);     \
+    cudaError_t launch_grad##S##_c##X##_2(const LaunchEnv& e, const GradArgs& a, cudaStream_t st);     \
+    cudaError_t launch_grad##S##_c##X##_3(const LaunchEnv& e, const GradArgs& a, cudaStream_t st);     \
+    cudaError_t launch_grad##S##_c##X##_4(const LaunchEnv& e, const GradArgs& a, cudaStream_t st);     \
+    cudaError_t launch_grad##S##_c##X##_5(const LaunchEnv& e, const GradArgs& a, cudaStream_t st);
 #define AIMD_DECLARE_CLASS(X)                                                                          \
     cudaError_t launch_schwarz_c##X(const LaunchEnv& e, const QuartetArgs& q, cudaStream_t st);         \
-    cudaError_t launch_jk_c##X(const LaunchEnv& e, const JKArgs& a, cudaStream_t st);                    \
-    cudaError_t launch_grad_c##X##_0(const LaunchEnv& e, const GradArgs& a, cudaStream_t st);          \
-    cudaError_t launch_grad_c##X##_1(const LaunchEnv& e, const GradArgs& a, cudaStream_t st);          \
-    cudaError_t launch_grad_c##X##_2(const LaunchEnv& e, const GradArgs& a, cudaStream_t st);          \
-    cudaError_t launch_grad_c##X##_3(const LaunchEnv& e, const GradArgs& a, cudaStream_t st);          \
-    cudaError_t launch_grad_c##X##_4(const LaunchEnv& e, const GradArgs& a, cudaStream_t st);          \
-    cudaError_t launch_grad_c##X##_5(const LaunchEnv& e, const GradArgs& a, cudaStream_t st);
+    AIMD_DECLARE_TYPED(X, )                                                                            \
+    AIMD_DECLARE_TYPED(X, 32)
 AIMD_DECLARE_CLASS(0)
 AIMD_DECLARE_CLASS(1)
 AIMD_DECLARE_CLASS(2)
@@ -38,6 +43,7 @@ AIMD_DECLARE_CLASS(3)
 AIMD_DECLARE_CLASS(4)
 AIMD_DECLARE_CLASS(5)
 #undef AIMD_DECLARE_CLASS
+#undef AIMD_DECLARE_TYPED
 
 cudaError_t launch_onee(const LaunchEnv& e, const ShellView& sv, const int* sp_cls_start, const double* origin,
                         double* S, double* T, double* M, double* V, cudaStream_t st, int* nlaunch);

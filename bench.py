@@ -4,7 +4,12 @@ Benchmark: MD steps/s (SCF + forces) of the Hartree-Fock hot path on B200.
 Workload (default, ``--workload h2o32``): (H2O)32 RHF/cc-pVDZ (Cartesian,
 800 AOs), 32 rigid waters at seeded random positions in a cube for
 1 g/cm^3, XL-BOMD (K = 5, dt = 0.5 fs), CSVR 300 K, tau = 100 fs, seed 1,
-FP64 kernels, default SCF thresholds (dE < 1e-10 Eh, commutator < 1e-7).
+default SCF thresholds (dE < 1e-10 Eh, commutator < 1e-7). Precision
+(``--precision``): "mixed" (default, the headline) evaluates quartets with
+Schwarz product Q1 Q2 < 1e-3 (``--fp32-cutoff``) in FP32 with FP64
+accumulation; the plain FP64 path is timed beside it in the same run, and
+the energy / force / dipole differences of the two at the starting geometry
+are reported (config.error_vs_fp64_at_start).
 One step = one MD step: XL-BOMD guess, SCF to convergence, analytic
 gradient, Verlet update. ``--workload methanol``: CH3OH RHF/6-31G**
 (50 AOs) NVE velocity Verlet at dt = 0.5 fs, 300 K initial velocities.
@@ -276,34 +281,27 @@ def run_reference_arm(args) -> None:
     }))
 
 
-def run_ours(args) -> None:
+def _md_path(args, sym, pos, vel, w, seed, ndof, fp32_cutoff, l2, dist, local, sample_clocks):
+    """Warm-up + K timed steps of the device-resident XL-BOMD loop at one precision."""
     import torch
 
     from aimd_b200 import md as MD
-    from aimd_b200.backend import HFGPUBackend
     from aimd_b200.engine import engine_for
     from aimd_b200.scf import SCFOptions, SCFSolver
 
-    rank, world, dist = _dist()
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    w = WORKLOADS[args.workload]
-    sym, pos = _geometry(w)
-    seed = 1 + rank
-    vel = MD.maxwell_boltzmann(sym, 300.0, seed)
-    ndof = 3 * len(sym) - 3
-    l2 = torch.empty(64 * 1024 * 1024, dtype=torch.float64, device="cuda")   # 512 MB > L2
-
-    # ---- value: device-resident MD loop
-    solver = SCFSolver(sym, w["basis"], options=SCFOptions(warn_unconverged=False))
+    solver = SCFSolver(sym, w["basis"], options=SCFOptions(warn_unconverged=False, fp32_cutoff=fp32_cutoff))
     thermo = MD.CSVR(300.0, 100.0, seed, ndof) if w["thermostat"] else None
     run = MD.DeviceXLBOMD(solver, sym, pos, vel, 0.5, k=5, thermostat=thermo)
+    st0 = run.state
+    start = {"energy": float(st0.energy), "gradient": run.gradient.detach().clone(),
+             "dipole": -torch.einsum("xmn,mn->x", st0.dipole_ints, st0.spin[0] + st0.spin[1])}
     for _ in range(args.warmup):
         run.step()
     eng = engine_for(run.state.basis)
     launches0 = eng.launch_count()
-    clocks = ClockSampler(local)
-    clocks.start()
+    clocks = ClockSampler(local) if sample_clocks else None
+    if clocks:
+        clocks.start()
     step_ms = []
     if dist is not None:
         dist.barrier()
@@ -319,33 +317,68 @@ def run_ours(args) -> None:
     torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
-    clk = clocks.stop()
+    clk = clocks.stop() if clocks else None
     launches = eng.launch_count() - launches0
     t_job = max_over_ranks(sum(step_ms) * 1e-3, dist)
-    steps_all = sum_over_ranks(float(args.steps), dist)
-    value = steps_all / t_job
-    iters = run.iterations[-args.steps:]
+    value = sum_over_ranks(float(args.steps), dist) / t_job
+    return {"value": value, "t_job": t_job, "iters": run.iterations[-args.steps:], "launches": launches,
+            "clocks": clk, "run": run, "start": start}
 
-    # ---- roofline of the J/K build at the last geometry and density
+
+def run_ours(args) -> None:
+    import torch
+
+    from aimd_b200 import md as MD
+    from aimd_b200.backend import HFGPUBackend
+    from aimd_b200.engine import engine_for
+
+    rank, world, dist = _dist()
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    w = WORKLOADS[args.workload]
+    sym, pos = _geometry(w)
+    seed = 1 + rank
+    vel = MD.maxwell_boltzmann(sym, 300.0, seed)
+    ndof = 3 * len(sym) - 3
+    l2 = torch.empty(64 * 1024 * 1024, dtype=torch.float64, device="cuda")   # 512 MB > L2
+    cutoff = args.fp32_cutoff if args.precision == "mixed" else 0.0
+
+    # ---- value: device-resident MD loop at the requested precision, and the
+    # plain FP64 path beside it (same trajectory start, same step count)
+    main = _md_path(args, sym, pos, vel, w, seed, ndof, cutoff, l2, dist, local, True)
+    ref64 = main if cutoff == 0.0 else _md_path(args, sym, pos, vel, w, seed, ndof, 0.0, l2, dist, local, False)
+    value = main["value"]
+    run = main["run"]
+    iters = main["iters"]
+    err = {"energy_eh": abs(main["start"]["energy"] - ref64["start"]["energy"]),
+           "force_eh_bohr": float((main["start"]["gradient"] - ref64["start"]["gradient"]).abs().max()),
+           "dipole_e_bohr": float((main["start"]["dipole"] - ref64["start"]["dipole"]).abs().max())}
+
+    # ---- roofline of the FP64 J/K build at the last geometry and density
     eng = engine_for(run.state.basis)
     D = (run.state.spin[0] + run.state.spin[1])[None].contiguous()
     flop, nq = flop_model_device(eng, run.state.basis)
-    eng.jk_acc(D, 1e-12)
-    jk_ms = []
-    for _ in range(3):
-        flush_l2(l2)
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record()
-        eng.jk_acc(D, 1e-12)
-        e.record()
-        e.synchronize()
-        jk_ms.append(s.elapsed_time(e))
-    jk_t = statistics.mean(jk_ms) * 1e-3
+
+    def build_ms(fp32_cutoff):
+        eng.jk_acc(D, 1e-12, fp32_cutoff)
+        ts = []
+        for _ in range(3):
+            flush_l2(l2)
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            eng.jk_acc(D, 1e-12, fp32_cutoff)
+            e.record()
+            e.synchronize()
+            ts.append(s.elapsed_time(e))
+        return statistics.mean(ts)
+
+    jk_t = build_ms(0.0) * 1e-3
+    jk_mixed_ms = build_ms(cutoff) if cutoff > 0.0 else None
     peak = fp64_peak_tflops()
     achieved = flop / jk_t / 1e12
 
-    # ---- e2e through the public API
-    backend = HFGPUBackend(sym, basis=w["basis"])
+    # ---- e2e through the public API (host numpy in and out)
+    backend = HFGPUBackend(sym, basis=w["basis"], scf_options={"fp32_cutoff": cutoff})
     thermo2 = MD.CSVR(300.0, 100.0, seed, ndof) if w["thermostat"] else None
     run2 = MD.XLBOMDRun(backend, sym, pos, vel, 0.5, k=5, thermostat=thermo2, xl=w["xl"])
     for _ in range(min(args.warmup, 2)):
@@ -367,26 +400,31 @@ def run_ours(args) -> None:
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        from oracle import hf_oracle as O
-        flop_t = flop
-        cpu = cpu_sample(float(np.mean(iters)), flop_t)
-        del O
+        cpu = cpu_sample(float(np.mean(iters)), flop)
     if rank == 0:
+        prec = (f"mixed: FP32 quartets for Q1 Q2 < {cutoff:g}, FP64 otherwise, FP64 accumulation"
+                if cutoff > 0.0 else "fp64 kernels")
         line = {
             "metric": METRIC, "value": value, "unit": "MD steps/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * t_job / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": w["desc"], "precision": "fp64 kernels", "l2": "flushed (512 MB write) before each step",
+            "warmup": args.warmup, "ms_per_step": 1e3 * main["t_job"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32" if cutoff > 0.0 else "f64",
+            "data": "synthetic",
+            "config": {"workload": w["desc"], "precision": prec, "l2": "flushed (512 MB write) before each step",
                        "parallelism": f"replicas{world}" if world > 1 else "single GPU",
-                       "scf_iterations_per_step": float(np.mean(iters))},
+                       "scf_iterations_per_step": float(np.mean(iters)),
+                       "fp64_path": {"value": ref64["value"], "ms_per_step": 1e3 * ref64["t_job"] / args.steps,
+                                     "scf_iterations_per_step": float(np.mean(ref64["iters"]))},
+                       "speedup_vs_fp64": value / ref64["value"],
+                       "error_vs_fp64_at_start": err},
             "e2e": {"value": e2e, "unit": "MD steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": None,
-                         "kernel": "integral-direct J/K build (jk_bra_kernel, 6 pair-class launches)",
+                         "kernel": "integral-direct FP64 J/K build (jk_bra_kernel, 6 pair-class launches)",
                          "model_flop_per_build": flop, "prim_quartets": nq, "build_ms": jk_t * 1e3,
+                         "mixed_build_ms": jk_mixed_ms,
                          "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64)"},
-            "gpu_launches": int(launches),
-            "clocks": clk,
+            "gpu_launches": int(main["launches"]),
+            "clocks": main["clocks"],
         }
         if cpu is not None:
             line["cpu_baseline"] = cpu
@@ -404,6 +442,10 @@ def main() -> None:
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="h2o32")
     ap.add_argument("--iters-per-step", type=float, default=8.0, help="reference arm: SCF iterations per MD step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed",
+                    help="mixed: FP32 for quartets with Q1 Q2 < --fp32-cutoff (the headline); the FP64 path "
+                         "is always timed beside it")
+    ap.add_argument("--fp32-cutoff", type=float, default=1e-3)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)

@@ -55,6 +55,14 @@ int aimd_set_geometry(aimd_ctx *ctx, const double *pos, void *stream);
 int aimd_schwarz(aimd_ctx *ctx, double *Q, void *stream);
 int aimd_pair_count(aimd_ctx *ctx);
 
+/* Mixed precision: quartets with Q1 Q2 < cutoff are evaluated in FP32
+ * (their contributions still accumulate in FP64, and the Boys function for
+ * T >= 40 stays FP64) by aimd_jk, aimd_jk_delta and aimd_grad2e on this
+ * context; cutoff 0 (the default) keeps every quartet in FP64. The
+ * reference is FP64 throughout; this implements the FP32-below-cutoff rule
+ * of the mixed-precision path, applied to the Schwarz product Q1 Q2. */
+int aimd_set_fp32_cutoff(aimd_ctx *ctx, double cutoff);
+
 /* Integral-direct J/K for nset symmetric densities D[nset][nao][nao]
  * (device). Writes the un-symmetrised accumulators: the caller forms
  * J = J + J^T and K = K + K^T. Quartets with Q1 Q2 < thr are skipped.

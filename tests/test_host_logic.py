@@ -54,6 +54,11 @@ def test_scf_options_and_electron_counts():
         SCFOptions(damping=1.0)
     with pytest.raises(ValueError):
         SCFOptions(fock_rebuild=0)
+    with pytest.raises(ValueError):
+        SCFOptions(fp32_cutoff=-1.0)
+    with pytest.raises(ValueError):
+        SCFOptions(fp32_cutoff=float("inf"))
+    assert SCFOptions().fp32_cutoff == 0.0
     assert SCFOptions().incremental_fock and SCFOptions(incremental_fock=False).fock_rebuild >= 1
     assert electron_counts(10, 0, 1, "rhf") == (5, 5)
     assert electron_counts(9, 0, 2) == (5, 4)
