@@ -57,6 +57,7 @@ struct BraStageT {
     const double* rec;      // bra primitive records (global)
     RT* E;                  // [nbp][BraE::SIZE] (shared)
     RT* SB;                 // [nbp][SBW] (shared)
+    RT* D;                  // gradients: [nbp][BraD::SIZE] derivative coefficients (shared)
 };
 using BraStage = BraStageT<double>;
 

@@ -32,6 +32,35 @@ struct GradArgs {
     int nblock;
 };
 
+// Bra derivative coefficients of one primitive pair, per direction d:
+//   k = 0 (centre A): 2a E^{i+1,j}_t - i E^{i-1,j}_t
+//   k = 1 (centre B): 2b E^{i,j+1}_t - j E^{i,j-1}_t
+// for i <= LA, j <= LB, t <= LA + LB + 1, staged once per CTA so that the
+// per-column derivative pass reads one value instead of building it.
+template <int LA, int LB>
+struct BraD {
+    static constexpr int I = LA + 1, J = LB + 1, T = LA + LB + 2;
+    static constexpr int SIZE = 2 * 3 * I * J * T;
+    __device__ static int at(int k, int d, int i, int j, int t) { return (((k * 3 + d) * I + i) * J + j) * T + t; }
+};
+
+template <int LA, int LB, typename RT>
+__device__ __forceinline__ void stage_bra_d(const BraStageT<RT>& st) {
+    using BE = BraE<LA, LB, 1>;
+    using BD = BraD<LA, LB>;
+    for (int w = threadIdx.x; w < st.nbp * BD::SIZE; w += blockDim.x) {
+        const int ib = w / BD::SIZE, r = w % BD::SIZE;
+        const int t = r % BD::T, j = (r / BD::T) % BD::J, i = (r / (BD::T * BD::J)) % BD::I;
+        const int d = (r / (BD::T * BD::J * BD::I)) % 3, k = r / (BD::T * BD::J * BD::I * 3);
+        const RT* E = st.E + (size_t)ib * BE::SIZE;
+        const RT* sb = st.SB + (size_t)ib * SBW;
+        RT v;
+        if (k == 0) v = RT(2) * sb[5] * E[BE::at(d, i + 1, j, t)] - (i > 0 ? i * E[BE::at(d, i - 1, j, t)] : RT(0));
+        else v = RT(2) * sb[6] * E[BE::at(d, i, j + 1, t)] - (j > 0 ? j * E[BE::at(d, i, j - 1, t)] : RT(0));
+        st.D[(size_t)ib * BD::SIZE + r] = v;
+    }
+}
+
 // For runtime (i, j): row[t] = E^{ij}_t and drow[t] = 2c E^{i+1,j}_t - i E^{i-1,j}_t
 // (the d/dC_x expansion), selected by predicated copies.
 template <int LC, int LD, typename RT>
@@ -58,6 +87,7 @@ __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStageT<R
                                             int id, int kg, double (&gab)[6], double* gsh) {
     using Q = QClass<CX, CY>;
     using BE = BraE<Q::LA, Q::LB, 1>;
+    using BD = BraD<Q::LA, Q::LB>;
     constexpr int LA = Q::LA, LB = Q::LB, LC = Q::LC, LD = Q::LD, LAB = Q::LAB, LCD = Q::LCD, L = Q::L + 1;
     constexpr int NH1 = nherm(LAB + 1);
     constexpr int UH = L >= 5 ? 1 : 16;      // rolled outer Hermite loops for large classes
@@ -134,11 +164,12 @@ __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStageT<R
         }
         for (int ib = 0; ib < st.nbp; ++ib) {
             const RT* sb = st.SB + ib * SBW;
-            const RT p = sb[0], ea = sb[5], eb = sb[6];
+            const RT p = sb[0];
             const RT rs = rsqrt_t(p + q);
             const RT alpha = p * q * rs * rs;
             const RT pref = RT(TWO_PI_2_5) * sb[1] * iq * rs;
             const RT* E = st.E + (size_t)ib * BE::SIZE;
+            const RT* Db = st.D + (size_t)ib * BD::SIZE;
             RT R[nherm(L)];
             hermite_r<L>(alpha, sb[2] - k.Qx, sb[3] - k.Qy, sb[4] - k.Qz, R);
             // Gamma contracted with this bra primitive's coefficients and f_ab,
@@ -207,19 +238,15 @@ __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStageT<R
                                 const RT yv = g * Xb[hidx(t, u, w)];
                                 const RT e0 = E[BE::at(0, ax, bx, t)], e1 = E[BE::at(1, ay, by, u)],
                                              e2 = E[BE::at(2, az, bz, w)];
-                                if (over == 0) Y[hidx(t, u, w)] += g * e0 * e1 * e2;
-                                const RT dax = RT(2) * ea * E[BE::at(0, ax + 1, bx, t)] - (ax > 0 ? ax * E[BE::at(0, ax > 0 ? ax - 1 : 0, bx, t)] : RT(0));
-                                const RT day = RT(2) * ea * E[BE::at(1, ay + 1, by, u)] - (ay > 0 ? ay * E[BE::at(1, ay > 0 ? ay - 1 : 0, by, u)] : RT(0));
-                                const RT daz = RT(2) * ea * E[BE::at(2, az + 1, bz, w)] - (az > 0 ? az * E[BE::at(2, az > 0 ? az - 1 : 0, bz, w)] : RT(0));
-                                const RT dbx = RT(2) * eb * E[BE::at(0, ax, bx + 1, t)] - (bx > 0 ? bx * E[BE::at(0, ax, bx > 0 ? bx - 1 : 0, t)] : RT(0));
-                                const RT dby = RT(2) * eb * E[BE::at(1, ay, by + 1, u)] - (by > 0 ? by * E[BE::at(1, ay, by > 0 ? by - 1 : 0, u)] : RT(0));
-                                const RT dbz = RT(2) * eb * E[BE::at(2, az, bz + 1, w)] - (bz > 0 ? bz * E[BE::at(2, az, bz > 0 ? bz - 1 : 0, w)] : RT(0));
-                                dA[0] += yv * dax * e1 * e2;
-                                dA[1] += yv * e0 * day * e2;
-                                dA[2] += yv * e0 * e1 * daz;
-                                dB[0] += yv * dbx * e1 * e2;
-                                dB[1] += yv * e0 * dby * e2;
-                                dB[2] += yv * e0 * e1 * dbz;
+                                const RT e12 = e1 * e2, e02 = e0 * e2, e01 = e0 * e1;
+                                if (over == 0) Y[hidx(t, u, w)] += g * e01 * e2;
+                                const RT y12 = yv * e12, y02 = yv * e02, y01 = yv * e01;
+                                dA[0] += y12 * Db[BD::at(0, 0, ax, bx, t)];
+                                dA[1] += y02 * Db[BD::at(0, 1, ay, by, u)];
+                                dA[2] += y01 * Db[BD::at(0, 2, az, bz, w)];
+                                dB[0] += y12 * Db[BD::at(1, 0, ax, bx, t)];
+                                dB[1] += y02 * Db[BD::at(1, 1, ay, by, u)];
+                                dB[2] += y01 * Db[BD::at(1, 2, az, bz, w)];
                             }
                 }
             }
@@ -322,6 +349,7 @@ __global__ void __launch_bounds__(128, AIMD_GRAD_MINB) grad2e_bra_kernel(GradArg
     const int spos = a.q.cls_start[CX] + blockIdx.x;
     if (threadIdx.x == 0) {
         load_stage(a.q, a.q.sorted[spos], st, Esm);
+        st.D = st.E + (size_t)st.nbp * BraE<Q0::LA, Q0::LB, 1>::SIZE;
         int64_t tot = 0;
         for (int sub = 0; sub < NSUB; ++sub) {
             int64_t kb, ke;
@@ -334,6 +362,8 @@ __global__ void __launch_bounds__(128, AIMD_GRAD_MINB) grad2e_bra_kernel(GradArg
     if (!any) return;
     for (int i = threadIdx.x; i < 3 * a.natm; i += blockDim.x) gsh[i] = 0.0;
     stage_bra_e<Q0::LA, Q0::LB, 1>(st);
+    __syncthreads();
+    stage_bra_d<Q0::LA, Q0::LB>(st);
     __syncthreads();
     double gab[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     int rot = 0;
@@ -351,7 +381,8 @@ __global__ void __launch_bounds__(128, AIMD_GRAD_MINB) grad2e_bra_kernel(GradArg
 template <int CX, typename RT>
 size_t grad_smem_bytes(int natm, int max_bra_prims) {
     using Q0 = QClass<CX, 0>;
-    return sizeof(double) * 3 * (size_t)natm + sizeof(RT) * (size_t)max_bra_prims * (BraE<Q0::LA, Q0::LB, 1>::SIZE + SBW);
+    return sizeof(double) * 3 * (size_t)natm +
+           sizeof(RT) * (size_t)max_bra_prims * (BraE<Q0::LA, Q0::LB, 1>::SIZE + BraD<Q0::LA, Q0::LB>::SIZE + SBW);
 }
 
 }  // namespace hf
