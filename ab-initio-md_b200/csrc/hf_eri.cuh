@@ -430,7 +430,10 @@ __device__ __forceinline__ void ket_items(int j0, int64_t cnt, KetQueue& q, int&
         const int items = q.n * NPER;
         int it = static_cast<int>(threadIdx.x) - rot;
         if (it < 0) it += blockDim.x;
-        for (; it < items; it += blockDim.x) work(q.pos[it / NPER], it % NPER);
+        // column-major: neighbouring lanes take the same ket column of
+        // different ket pairs, so the column's box conditions are warp-uniform
+        const int nq = q.n;
+        for (; it < items; it += blockDim.x) work(q.pos[it % nq], it / nq);
         rot = (rot + items) % static_cast<int>(blockDim.x);
         __syncthreads();
     }
