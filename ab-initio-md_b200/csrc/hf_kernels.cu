@@ -80,6 +80,7 @@ struct aimd_ctx {
     // (0: all FP64); counts_hi is the FP64 prefix table, built at thr_hi
     double fp32_cutoff = 0.0, thr_hi = -1.0;
     int64_t* counts_hi;
+    int64_t* counts_hi_d;   // difference builds: FP64 prefix at fp32_cutoff / max|dD| (per call)
     void* cub_tmp;
     size_t cub_bytes;
     double* pos;            // [natm][3] device copy of the current geometry
@@ -214,6 +215,7 @@ extern "C" int aimd_create(aimd_ctx** out, int natm, int nao, int nblock, const 
         CK(dalloc(&c->counts_jk, (size_t)NSEG * (np + 1)));
         CK(dalloc(&c->counts_g, (size_t)NSEG * (np + 1)));
         CK(dalloc(&c->counts_d, (size_t)NSEG * (np + 1)));
+        CK(dalloc(&c->counts_hi_d, (size_t)NSEG * (np + 1)));
         CK(dalloc(&c->counts_hi, (size_t)NSEG * (np + 1)));
         CK(dalloc(&c->bmax, (size_t)nblock * nblock));
         CK(dalloc(&c->dmax, 1));
@@ -243,7 +245,7 @@ extern "C" int aimd_destroy(aimd_ctx* c) {
                     c->sh_atom, c->sh_l, c->sh_ao, c->sh_p0, c->sh_np, c->sp_i, c->sp_j, c->sh_exp, c->sh_coef,
                     c->charges, c->pa, c->pb, c->npp, c->slot, c->rec, c->Q, c->by_class, c->idx_in,
                     c->tmp_idx, c->seg_id, c->seg_keys, c->seg_keys_out, c->seg_start, c->tmpQ, c->sortedQ,
-                    c->sorted, c->counts_jk, c->counts_g, c->counts_d, c->bmax, c->dmax, c->bmc, c->bmx, c->counts_hi, c->cub_tmp, c->pos};
+                    c->sorted, c->counts_jk, c->counts_g, c->counts_d, c->bmax, c->dmax, c->bmc, c->bmx, c->counts_hi, c->counts_hi_d, c->cub_tmp, c->pos};
     for (void* p : ptrs) cudaFree(p);
     for (int i = 0; i < NCLS; ++i) {
         if (c->cls_stream[i]) cudaStreamDestroy(c->cls_stream[i]);
@@ -664,8 +666,14 @@ extern "C" int aimd_jk_delta(aimd_ctx* c, int nset, const double* D, double* J, 
     // enumerate at max(thr, dthr / max|D|): the integral screen still holds,
     // and no quartet that the density-weighted test keeps is missed
     if (int r = build_counts(c, dthr, c->counts_d, st, c->dmax, thr)) return r;
+    // mixed precision: a quartet of a difference build contributes at most
+    // Q1 Q2 max|dD|, so the FP32 rule is applied to that product, i.e. the
+    // FP64 prefix is cut at fp32_cutoff / max|dD|
     const int64_t* hi = nullptr;
-    if (int r = hi_counts(c, st, &hi)) return r;
+    if (c->fp32_cutoff > 0.0) {
+        if (int r = build_counts(c, c->fp32_cutoff, c->counts_hi_d, st, c->dmax, 0.0)) return r;
+        hi = c->counts_hi_d;
+    }
     const bool mixed = hi != nullptr;
     CK(cudaMemsetAsync(J, 0, sizeof(double) * nset * nn, st));
     CK(cudaMemsetAsync(K, 0, sizeof(double) * nset * nn, st));
