@@ -83,3 +83,10 @@ def test_random_molecules_are_valid():
         sym, pos = G.random_molecule(seed)
         assert 3 <= len(sym) <= 20
         assert set(sym) <= {"H", "C", "N", "O"}
+
+
+def test_batch_default_multiplicity():
+    from aimd_b200.batch import default_multiplicity
+    assert default_multiplicity(["O", "H", "H"]) == 1
+    assert default_multiplicity(["C", "H", "H", "H"]) == 2
+    assert default_multiplicity(["C", "H", "H", "H"], charge=1) == 1
