@@ -4,7 +4,7 @@ implementation (Nathan-W123/Ab-Initio-MD, numba CPU code) on the benchmark
 geometries. The reference is importable only where its source tree is
 available, so the fixtures are committed and the tests read them.
 
-    NUMBA_CACHE_DIR=/tmp/numba_cache python tests/golden/make_golden.py /path/to/reference
+    NUMBA_CACHE_DIR=/tmp/numba_cache python tests/golden/make_golden.py /path/to/reference [--only=case1,case2]
 
 Fixtures (all arrays float64, Hartree atomic units):
   boys.npz            F_0..F_32 at 60 arguments (aimd/qc/boys.py:143)
@@ -19,8 +19,11 @@ from __future__ import annotations
 
 import os
 import sys
+import zlib
 
 import numpy as np
+
+ANG = 1.8897261254578281          # bohr per angstrom
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
@@ -55,7 +58,10 @@ def _flop_model(basis, Q, pr, threshold):
 
 
 def main() -> None:
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    args = [a for a in sys.argv[1:] if not a.startswith("--only=")]
+    only = [a.split("=", 1)[1].split(",") for a in sys.argv[1:] if a.startswith("--only=")]
+    only = set(only[0]) if only else None
+    ref = args[0] if args else "/root/reference"
     sys.path.insert(0, ref)
     sys.path.insert(0, os.path.join(REPO, "ab-initio-md_b200"))
     from aimd.qc import integrals as I
@@ -68,8 +74,9 @@ def main() -> None:
     rng = np.random.default_rng(2024)
     xs = np.concatenate([10 ** rng.uniform(-8, np.log10(150.0), 50),
                          [0.0, 0.05, 1.0, 39.999999, 40.0, 40.000001, 100.0, 1e3, 1e6, 1e12]])
-    F = np.array([boys(32, float(x)) for x in xs])
-    np.savez_compressed(os.path.join(HERE, "boys.npz"), x=xs, F=F)
+    if only is None:
+        F = np.array([boys(32, float(x)) for x in xs])
+        np.savez_compressed(os.path.join(HERE, "boys.npz"), x=xs, F=F)
 
     cases = {
         "water_631gs": (*G.water(), "6-31g*", 0, 1, {}),
@@ -79,8 +86,17 @@ def main() -> None:
             [[0.0, 0.0, 0.0], [2.0598, 0.0, 0.0], [-1.0299, 1.7839, 0.0], [-1.0299, -1.7839, 0.3]]),
             "6-31g*", 0, 2, {}),
         "h2o8_ccpvdz": (*G.water_cluster(8, seed=0), "cc-pvdz", 0, 1, {"max_nao": 200}),
+        # second-row atoms: more primitives and general contractions of 3 s /
+        # 2 p columns per block in cc-pVDZ (split into smaller blocks on the device)
+        "h2s_631gs": (["S", "H", "H"], _bent(1.336, 92.1), "6-31g*", 0, 1, {}),
+        "hcl_ccpvdz": (["Cl", "H"], np.array([[0.0, 0.0, 0.0], [0.0, 0.0, 1.2746 * ANG]]), "cc-pvdz", 0, 1, {}),
     }
+    own_rng = {"h2s_631gs", "hcl_ccpvdz"}     # cases added later draw from their own generator
     for name, (sym, pos, basis, charge, mult, opts) in cases.items():
+        if only is not None and name not in only:
+            continue
+        if name in own_rng:
+            rng = np.random.default_rng(zlib.crc32(name.encode()))
         print(name, flush=True)
         b = build_basis(sym, pos, basis)
         pr = I._pairs(b)
@@ -128,6 +144,13 @@ def main() -> None:
             out["W"] = energy_weighted_density(res.spin_densities, res.fock)
         print(f"  nao {n} E {res.energy:.12f} it {res.iterations} flop {flop:.3e}", flush=True)
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+
+
+def _bent(r_ang: float, angle_deg: float) -> np.ndarray:
+    """X-H2 at r (A) and H-X-H angle (deg), X at the origin, bohr."""
+    t = np.radians(angle_deg) / 2
+    r = r_ang * ANG
+    return np.array([[0.0, 0.0, 0.0], [r * np.sin(t), 0.0, r * np.cos(t)], [-r * np.sin(t), 0.0, r * np.cos(t)]])
 
 
 if __name__ == "__main__":

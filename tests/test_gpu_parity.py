@@ -13,7 +13,7 @@ from oracle import hf_oracle as O
 
 pytestmark = pytest.mark.gpu
 
-CASES = ["water_631gs", "water_ccpvdz", "methanol_631gss", "ch3_uhf_631gs"]
+CASES = ["water_631gs", "water_ccpvdz", "methanol_631gss", "ch3_uhf_631gs", "h2s_631gs", "hcl_ccpvdz"]
 ERI_TOL = 1e-10
 E_TOL = 1e-9
 F_TOL = 1e-7

@@ -19,7 +19,7 @@ def test_boys_matches_reference(golden):
         np.testing.assert_allclose(O.boys(32, float(x)), F, rtol=1e-14, atol=1e-300)
 
 
-@pytest.mark.parametrize("case", ["water_631gs", "water_ccpvdz", "methanol_631gss", "ch3_uhf_631gs"])
+@pytest.mark.parametrize("case", ["water_631gs", "water_ccpvdz", "methanol_631gss", "ch3_uhf_631gs", "h2s_631gs", "hcl_ccpvdz"])
 def test_integrals_match_reference(golden, case):
     g = golden(case)
     b = _basis(g)
@@ -44,7 +44,7 @@ def test_integrals_match_reference(golden, case):
     np.testing.assert_allclose(O.one_electron_gradient(b, g["D_rand"], g["W_rand"]), g["g1e"], atol=1e-11)
 
 
-@pytest.mark.parametrize("case", ["water_631gs", "water_ccpvdz", "methanol_631gss", "ch3_uhf_631gs"])
+@pytest.mark.parametrize("case", ["water_631gs", "water_ccpvdz", "methanol_631gss", "ch3_uhf_631gs", "h2s_631gs", "hcl_ccpvdz"])
 def test_scf_energy_and_gradient_match_reference(golden, case):
     g = golden(case)
     sym = [str(s) for s in g["symbols"]]
