@@ -30,7 +30,7 @@ def _ncon_cap(l: int) -> int:
 
 def device_blocks(basis: BasisSet) -> dict:
     """Block arrays for the device, splitting over-cap general contractions."""
-    atom, lval, ncon, ao, p0, npr, exps, coefs = [], [], [], [], [], [], [], []
+    atom, lval, ncon, ao, p0, npr, exps, coefs, orig = [], [], [], [], [], [], [], [], []
     split = False
     for b in range(basis.nblock):
         l = int(basis.blk_l[b])
@@ -45,6 +45,7 @@ def device_blocks(basis: BasisSet) -> dict:
             rows = [k for k in range(k0, k1) if any(basis.blk_coef[k, c] != 0.0 for c in cols)] if len(cols) < nc \
                 else list(range(k0, k1))
             atom.append(int(basis.blk_atom[b]))
+            orig.append(b)
             lval.append(l)
             ncon.append(len(cols))
             ao.append(int(basis.blk_ao[b]) + c0 * nct)
@@ -56,7 +57,8 @@ def device_blocks(basis: BasisSet) -> dict:
     i32 = lambda v: np.ascontiguousarray(np.array(v, dtype=np.int32))  # noqa: E731
     return {"atom": i32(atom), "l": i32(lval), "ncon": i32(ncon), "ao": i32(ao), "p0": i32(p0), "np": i32(npr),
             "exp": np.ascontiguousarray(np.array(exps, dtype=float)),
-            "coef": np.ascontiguousarray(np.array(coefs, dtype=float).reshape(-1, 2)), "split": split}
+            "coef": np.ascontiguousarray(np.array(coefs, dtype=float).reshape(-1, 2)), "split": split,
+            "orig": np.array(orig, dtype=np.int64)}
 
 
 def _p32(a):

@@ -44,9 +44,24 @@ def _check_sym(D: np.ndarray, nao: int, what: str) -> np.ndarray:
 # ---------------------------------------------------------------- two-electron
 
 def schwarz_bounds(basis: BasisSet) -> np.ndarray:
-    """Q_P = max_ab |(ab|ab)|^(1/2) per block pair P = i(i+1)/2 + j (i >= j)."""
+    """
+    Q_P = max_ab |(ab|ab)|^(1/2) per block pair P = i(i+1)/2 + j (i >= j) of
+    the basis's blocks (aimd/qc/integrals.py:970). Blocks whose general
+    contraction the device splits are mapped back: the Q of a block pair is
+    the maximum over its device sub-pairs.
+    """
     eng = engine_for(basis)
-    return eng.schwarz().cpu().numpy()
+    Qd = eng.schwarz().cpu().numpy()
+    if not eng.split:
+        return Qd
+    orig = eng.blocks["orig"]
+    nd = len(orig)
+    i, j = np.tril_indices(nd)                      # device pair index i(i+1)/2 + j in row-major order
+    I_, J_ = orig[i], orig[j]
+    P = I_ * (I_ + 1) // 2 + J_
+    Q = np.zeros(basis.nblock * (basis.nblock + 1) // 2)
+    np.maximum.at(Q, P, Qd[i * (i + 1) // 2 + j])
+    return Q
 
 
 def eri_tensor(basis: BasisSet, schwarz_threshold: float = DEFAULT_SCHWARZ, max_nao: int = MAX_NAO_ERI) -> np.ndarray:
