@@ -34,14 +34,32 @@ using RT = float;
 #define AIMD_JK_NAME AIMD_CAT(launch_jk32_c, AIMD_CLASS)
 #endif
 
+template <int YK>
+cudaError_t launch_one(const LaunchEnv& e, const JKArgs& a, cudaStream_t st, size_t smem) {
+    cudaError_t r = set_smem_limit((const void*)jk_bra_kernel<CX, 1, RT, YK>, smem);
+    if (r != cudaSuccess) return r;
+    jk_bra_kernel<CX, 1, RT, YK><<<e.cls_count[CX], JK_THREADS, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+// split bra classes: one launch per non-empty ket class (largest first), in
+// order on st; the others: one launch over all ket classes
 cudaError_t AIMD_JK_NAME(const LaunchEnv& e, const JKArgs& a, cudaStream_t st) {
     const int cnt = e.cls_count[CX];
     if (cnt == 0) return cudaSuccess;
     const size_t smem = jk_smem_bytes<CX, 1, RT>(e.nao, e.maxbp[CX]);
-    cudaError_t r = set_smem_limit((const void*)jk_bra_kernel<CX, 1, RT>, smem);
-    if (r != cudaSuccess) return r;
-    jk_bra_kernel<CX, 1, RT><<<cnt * JKKernel<CX, 1>::NY, JK_THREADS, smem, st>>>(a);
-    return cudaGetLastError();
+    if constexpr (!JKKernel<CX, 1>::SPLIT) {
+        return launch_one<-1>(e, a, st, smem);
+    } else {
+        cudaError_t r = cudaSuccess;
+        if constexpr (CX >= 5) if (r == cudaSuccess && e.cls_count[5]) r = launch_one<5>(e, a, st, smem);
+        if constexpr (CX >= 4) if (r == cudaSuccess && e.cls_count[4]) r = launch_one<4>(e, a, st, smem);
+        if (r == cudaSuccess && e.cls_count[3]) r = launch_one<3>(e, a, st, smem);
+        if (r == cudaSuccess && e.cls_count[2]) r = launch_one<2>(e, a, st, smem);
+        if (r == cudaSuccess && e.cls_count[1]) r = launch_one<1>(e, a, st, smem);
+        if (r == cudaSuccess && e.cls_count[0]) r = launch_one<0>(e, a, st, smem);
+        return r;
+    }
 }
 
 }  // namespace hf

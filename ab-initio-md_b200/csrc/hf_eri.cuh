@@ -490,8 +490,10 @@ struct JKKernel {
     static constexpr int NROW = Q0::NROW;
     static constexpr int NF = Q0::KA * Q0::NA + Q0::KB * Q0::NB;
     static constexpr int ESIZE = BraE<Q0::LA, Q0::LB, 0>::SIZE;
-    // d-bra classes: one CTA per (bra pair, ket class), shorter CTAs that
-    // fill the machine; dd bras accumulate K in global memory
+    // d-bra classes: one kernel per ket class (one CTA per bra pair each):
+    // shorter CTAs that fill the machine, and each kernel holds the code of
+    // one ket class only, so the CTAs resident on an SM share their
+    // instructions; dd bras accumulate K in global memory
     static constexpr bool SPLIT = CX >= 3;
     static constexpr int NY = SPLIT ? CX + 1 : 1;
     static constexpr bool KGLOBAL = CX == 5;
@@ -504,10 +506,11 @@ constexpr int JK_THREADS = 128;
 
 // RT = double: the FP64 quartets; RT = float: the FP32 quartets of the
 // mixed-precision path (their J/K contributions still accumulate in FP64).
+// YK = ket class of this kernel, or -1: every ket class in each CTA.
 #ifndef AIMD_JK_MINB
 #define AIMD_JK_MINB 1
 #endif
-template <int CX, int NS, typename RT>
+template <int CX, int NS, typename RT, int YK>
 __global__ void __launch_bounds__(JK_THREADS, AIMD_JK_MINB) jk_bra_kernel(JKArgs a) {
     using KK = JKKernel<CX, NS>;
     using Q0 = QClass<CX, 0>;
@@ -516,8 +519,8 @@ __global__ void __launch_bounds__(JK_THREADS, AIMD_JK_MINB) jk_bra_kernel(JKArgs
     double* Ksm = smem;
     double* Jt = Ksm + (size_t)KK::KROWS * n;
     RT* Esm = reinterpret_cast<RT*>(Jt + NS * KK::NROW * JK_THREADS);
-    const int yk = KK::SPLIT ? (int)(blockIdx.x % KK::NY) : -1;
-    const int spos = a.q.cls_start[CX] + (int)(blockIdx.x / KK::NY);
+    constexpr int yk = YK;
+    const int spos = a.q.cls_start[CX] + (int)blockIdx.x;
     const int P1 = a.q.sorted[spos];
     __shared__ BraStageT<RT> st;
     __shared__ KetQueue kq;
@@ -541,12 +544,12 @@ __global__ void __launch_bounds__(JK_THREADS, AIMD_JK_MINB) jk_bra_kernel(JKArgs
     __syncthreads();
     constexpr bool KG_ = KK::KGLOBAL;
     int rot = 0;
-    if (yk < 0 || yk == 0) jk_ket_class<CX, 0, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot);
-    if constexpr (CX >= 1) if (yk < 0 || yk == 1) jk_ket_class<CX, 1, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot);
-    if constexpr (CX >= 2) if (yk < 0 || yk == 2) jk_ket_class<CX, 2, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot);
-    if constexpr (CX >= 3) if (yk < 0 || yk == 3) jk_ket_class<CX, 3, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot);
-    if constexpr (CX >= 4) if (yk < 0 || yk == 4) jk_ket_class<CX, 4, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot);
-    if constexpr (CX >= 5) if (yk < 0 || yk == 5) jk_ket_class<CX, 5, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot);
+    if constexpr (yk < 0 || yk == 0) jk_ket_class<CX, 0, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot);
+    if constexpr (CX >= 1 && (yk < 0 || yk == 1)) jk_ket_class<CX, 1, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot);
+    if constexpr (CX >= 2 && (yk < 0 || yk == 2)) jk_ket_class<CX, 2, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot);
+    if constexpr (CX >= 3 && (yk < 0 || yk == 3)) jk_ket_class<CX, 3, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot);
+    if constexpr (CX >= 4 && (yk < 0 || yk == 4)) jk_ket_class<CX, 4, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot);
+    if constexpr (CX >= 5 && (yk < 0 || yk == 5)) jk_ket_class<CX, 5, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot);
     __syncthreads();
     const size_t nn = (size_t)n * n;
     // flush J_ab: one thread per (set, row) sums the per-thread slots

@@ -470,7 +470,15 @@ cudaError_t launch_grad_class(const LaunchEnv& e, const GradArgs& a, cudaStream_
 // kernel launches of one class step: J/K one per type, the gradient one
 // per (bra class, non-empty ket class) and type
 int cls_size(aimd_ctx* c, int cl) { return c->cls_start[cl + 1] - c->cls_start[cl]; }
-int jk_launches(aimd_ctx* c, int cl, bool mixed) { return cls_size(c, cl) > 0 ? (mixed ? 2 : 1) : 0; }
+int jk_launches(aimd_ctx* c, int cl, bool mixed) {
+    if (cls_size(c, cl) == 0) return 0;
+    int n = 1;
+    if (cl >= 3) {          // split bra classes: one kernel per non-empty ket class
+        n = 0;
+        for (int y = 0; y <= cl; ++y) n += cls_size(c, y) > 0 ? 1 : 0;
+    }
+    return mixed ? 2 * n : n;
+}
 int grad_launches(aimd_ctx* c, int cl, bool mixed) {
     int n = 0;
     for (int y = 0; y <= cl; ++y) n += (cls_size(c, cl) > 0 && cls_size(c, y) > 0) ? 1 : 0;
