@@ -490,11 +490,11 @@ struct JKKernel {
     static constexpr int NROW = Q0::NROW;
     static constexpr int NF = Q0::KA * Q0::NA + Q0::KB * Q0::NB;
     static constexpr int ESIZE = BraE<Q0::LA, Q0::LB, 0>::SIZE;
-    // d-bra classes: one kernel per ket class (one CTA per bra pair each):
-    // shorter CTAs that fill the machine, and each kernel holds the code of
-    // one ket class only, so the CTAs resident on an SM share their
+    // bra classes above ss: one kernel per ket class (one CTA per bra pair
+    // each): shorter CTAs that fill the machine, and each kernel holds the
+    // code of one ket class only, so the CTAs resident on an SM share their
     // instructions; dd bras accumulate K in global memory
-    static constexpr bool SPLIT = CX >= 3;
+    static constexpr bool SPLIT = CX >= 1;
     static constexpr int NY = SPLIT ? CX + 1 : 1;
     static constexpr bool KGLOBAL = CX == 5;
     static constexpr int KROWS = KGLOBAL ? 0 : NS * NF;

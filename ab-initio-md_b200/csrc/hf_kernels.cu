@@ -473,7 +473,7 @@ int cls_size(aimd_ctx* c, int cl) { return c->cls_start[cl + 1] - c->cls_start[c
 int jk_launches(aimd_ctx* c, int cl, bool mixed) {
     if (cls_size(c, cl) == 0) return 0;
     int n = 1;
-    if (cl >= 3) {          // split bra classes: one kernel per non-empty ket class
+    if (cl >= 1) {          // split bra classes: one kernel per non-empty ket class
         n = 0;
         for (int y = 0; y <= cl; ++y) n += cls_size(c, y) > 0 ? 1 : 0;
     }
