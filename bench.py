@@ -419,7 +419,7 @@ def run_ours(args) -> None:
             "e2e": {"value": e2e, "unit": "MD steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": None,
-                         "kernel": "integral-direct FP64 J/K build (jk_bra_kernel, 6 pair-class launches)",
+                         "kernel": "integral-direct FP64 J/K build (jk_bra_kernel, one launch per (bra, ket) pair class)",
                          "model_flop_per_build": flop, "prim_quartets": nq, "build_ms": jk_t * 1e3,
                          "mixed_build_ms": jk_mixed_ms,
                          "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64)"},
