@@ -1,7 +1,7 @@
 """
 Many geometries at once: SCF + analytic gradient for a list of molecules of
-uneven size (BASELINE's batched configuration: 64 random H/C/N/O molecules of
-3-20 atoms in 6-31G*).
+uneven size (the batched benchmark configuration: 64 random H/C/N/O
+molecules of 3-20 atoms in 6-31G*).
 
 Each molecule is small (tens to ~150 AOs), so one molecule at a time leaves
 most of the 148 SMs idle: its class kernels have a few dozen CTAs. The batch

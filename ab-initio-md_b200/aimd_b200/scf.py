@@ -735,7 +735,7 @@ class SCFSolver:
         spin = torch.stack([Ds[0], Ds[-1]])
         P = spin[0] + spin[1]
         q = torch.as_tensor(basis.nuclear_charges.copy(), device=S.device)
-        q = q.index_add(0, torch.as_tensor(basis.ao_atom, device=S.device), -torch.diagonal(P @ S))
+        q = q.index_add(0, torch.as_tensor(np.array(basis.ao_atom), device=S.device), -torch.diagonal(P @ S))
         dip = -torch.einsum("xmn,mn->x", Ik.M, P)
         sz = 0.5 * (self.n_alpha - self.n_beta)
         s2 = sz * (sz + 1.0) + self.n_beta - float(torch.sum((spin[0] @ S) * (spin[1] @ S).T)) if nspin == 2 else 0.0
