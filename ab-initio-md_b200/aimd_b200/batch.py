@@ -95,7 +95,7 @@ class BatchSolver:
             g = scf_gradient_device(st, fp32_cutoff=self.options.fp32_cutoff)
             dip = -torch.einsum("xmn,mn->x", st.dipole_ints, st.spin[0] + st.spin[1])
             g_h, dip_h = g.cpu().numpy(), dip.cpu().numpy()
-        basis = solver.basis
+        basis = st.basis                     # the basis at this call's positions
         dip_h = dip_h + (basis.nuclear_charges[:, None] * basis.positions).sum(axis=0)
         return BatchResult(st.energy, g_h, st.converged, st.iterations, dip_h, {"nao": solver.nao})
 

@@ -37,7 +37,10 @@ def test_batch_matches_backend_and_reruns():
     r = HFGPUBackend(sym, basis="6-31g*", multiplicity=default_multiplicity(sym)).compute(pos)
     assert abs(res[1].energy - r.energy) < 1e-9
     np.testing.assert_allclose(res[1].gradient, r.gradient, atol=1e-7)
+    np.testing.assert_allclose(res[1].dipole, r.dipole, atol=1e-6)
     moved = [p + 0.01 for _, p in mols]            # rigid shift: same energies
     res2 = bs.run(moved)
     for a, b in zip(res, res2):
         assert abs(a.energy - b.energy) < 1e-8
+        # the dipole of a neutral molecule does not depend on the origin
+        np.testing.assert_allclose(a.dipole, b.dipole, atol=1e-6)
