@@ -90,3 +90,15 @@ def test_batch_default_multiplicity():
     assert default_multiplicity(["O", "H", "H"]) == 1
     assert default_multiplicity(["C", "H", "H", "H"]) == 2
     assert default_multiplicity(["C", "H", "H", "H"], charge=1) == 1
+
+
+def test_autograd_and_batch_argument_checks():
+    import torch
+    from aimd_b200.autograd import scf_energy
+    from aimd_b200.batch import BatchSolver
+    with pytest.raises(TypeError):
+        scf_energy(np.zeros((3, 3)), None)                     # not a tensor
+    with pytest.raises(ValueError):
+        scf_energy(torch.zeros(3, 2, dtype=torch.float64), None)   # not (natm, 3)
+    with pytest.raises(ValueError):
+        BatchSolver([], workers=0)
