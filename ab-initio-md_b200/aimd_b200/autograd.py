@@ -23,6 +23,7 @@ import numpy as np
 import torch
 
 from .gradients import scf_gradient_device
+from .integrals import DEFAULT_SCHWARZ_GRAD
 from .scf import DeviceSCFState, SCFSolver, run_device
 
 
@@ -30,36 +31,40 @@ class SCFEnergyFunction(torch.autograd.Function):
     """E(R) forward by the device SCF, dE/dR backward by the gradient kernels."""
 
     @staticmethod
-    def forward(ctx, positions: torch.Tensor, solver: SCFSolver, guess, holder: dict):
+    def forward(ctx, positions: torch.Tensor, solver: SCFSolver, guess, holder: dict, screening: float):
         x = positions.detach().to("cpu", torch.float64).numpy().reshape(-1, 3)
         state = run_device(solver, x, guess)
         holder["state"] = state
         ctx.state = state
         ctx.fp32_cutoff = solver.options.fp32_cutoff
+        ctx.screening = screening
         return torch.tensor(state.energy, dtype=torch.float64, device=positions.device)
 
     @staticmethod
     def backward(ctx, grad_energy: torch.Tensor):
         if ctx.state is None:
             raise RuntimeError("scf_energy: backward called twice (only first derivatives are available)")
-        g = scf_gradient_device(ctx.state, fp32_cutoff=ctx.fp32_cutoff)
+        g = scf_gradient_device(ctx.state, ctx.screening, fp32_cutoff=ctx.fp32_cutoff)
         ctx.state = None
-        return grad_energy * g.to(grad_energy.device, torch.float64), None, None, None
+        return grad_energy * g.to(grad_energy.device, torch.float64), None, None, None, None
 
 
 def scf_energy(positions: torch.Tensor, solver: SCFSolver, guess: torch.Tensor | None = None,
-               holder: dict | None = None) -> torch.Tensor:
+               holder: dict | None = None, gradient_screening: float = DEFAULT_SCHWARZ_GRAD) -> torch.Tensor:
     """
     SCF energy (Eh, 0-d float64 tensor) at ``positions`` ((natm, 3) bohr,
     any device), differentiable with respect to ``positions``. ``guess``: a
     device density to start from (as run_device); ``holder``, if given,
-    receives the converged DeviceSCFState under "state".
+    receives the converged DeviceSCFState under "state";
+    ``gradient_screening``: the backward pass's threshold on
+    Q1 Q2 max|Gamma| (the reference's two-electron gradient screening).
     """
     if not isinstance(positions, torch.Tensor):
         raise TypeError("positions must be a torch.Tensor")
     if positions.dim() != 2 or positions.shape[1] != 3:
         raise ValueError(f"positions must have shape (natm, 3), got {tuple(positions.shape)}")
-    return SCFEnergyFunction.apply(positions, solver, guess, {} if holder is None else holder)
+    return SCFEnergyFunction.apply(positions, solver, guess, {} if holder is None else holder,
+                                   float(gradient_screening))
 
 
 class HFEnergy:

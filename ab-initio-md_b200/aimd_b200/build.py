@@ -16,6 +16,7 @@ import concurrent.futures as cf
 import glob
 import os
 import subprocess
+import time
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -72,8 +73,17 @@ def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -
     todo = [u for u in _units() if force or not os.path.exists(u[1]) or os.path.getmtime(u[1]) < newest]
     logs = []
     if todo:
+        # objects are stamped with the time the build started, so a source
+        # edited while they compile is newer than them and the next build
+        # compiles them again
+        start = time.time()
+
+        def one(u):
+            log = _compile(u, verbose)
+            os.utime(u[1], (start, start))
+            return log
         with cf.ThreadPoolExecutor(max_workers=jobs or min(len(todo), os.cpu_count() or 4)) as ex:
-            logs = list(ex.map(lambda u: _compile(u, verbose), todo))
+            logs = list(ex.map(one, todo))
     if todo or not os.path.exists(LIB):
         objs = [u[1] for u in _units()]
         res = subprocess.run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", LIB],

@@ -11,7 +11,7 @@ reference keeps them in ``aimd/qc/basis_data.py`` (``BASIS_SETS``,
 
 Run once, in a checkout that has the reference importable:
 
-    python make_basis_data.py /path/to/reference
+    python make_basis_data.py <reference source tree>
 """
 
 from __future__ import annotations
@@ -22,8 +22,9 @@ import sys
 
 
 def main() -> None:
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-    sys.path.insert(0, ref)
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_basis_data.py <reference source tree>")
+    sys.path.insert(0, sys.argv[1])
     from aimd.qc.basis_data import BASIS_SETS  # noqa: E402  (reference module)
 
     out = {}

@@ -133,18 +133,24 @@ class XLBOMDRun:
 class DeviceXLBOMD:
     """
     The same velocity Verlet + CSVR + XL-BOMD scheme with the auxiliary
-    density history, the SCF densities and the gradient kept on the device;
-    only positions (natm x 3) and scalars cross to the host.
+    density history and the SCF densities kept on the device; only positions
+    (natm x 3), forces and scalars cross to the host. Forces come from the
+    differentiable SCF energy (aimd_b200.autograd.scf_energy): the forward
+    pass is the device SCF from the XL-BOMD guess, the backward pass the
+    derivative kernels (autograd=True, the default), or from the analytic
+    gradient called directly (autograd=False; the same kernels).
     """
 
     def __init__(self, solver, symbols, positions, velocities, timestep_fs: float, k: int = 5,
-                 thermostat: CSVR | None = None, gradient_screening: float = 1e-14) -> None:
+                 thermostat: CSVR | None = None, gradient_screening: float = 1e-14, autograd: bool = True) -> None:
         import torch
 
         from .gradients import scf_gradient_device
         from .scf import run_device
         self._run, self._grad = run_device, scf_gradient_device
         self.torch = torch
+        self.autograd = autograd
+        self.phase_events = None
         self.solver = solver
         self.m = masses_au(symbols)
         self.x = np.array(positions, dtype=float)
@@ -155,14 +161,42 @@ class DeviceXLBOMD:
         self.fp32_cutoff = solver.options.fp32_cutoff
         kappa, alpha, c = XL_COEFFICIENTS[k]
         self.kappa, self.alpha, self.c = kappa, alpha, [float(v) for v in c]
-        self.state = self._run(solver, self.x, None)
-        self.gradient = self._grad(self.state, self.thr, self.fp32_cutoff)
+        self.state, self.gradient = self._forces(None)
         D = self._density(self.state)
         self.history = [D.clone() for _ in range(k + 1)]
         self.iterations = [self.state.iterations]
 
     def _density(self, st):
         return st.spin if st.unrestricted else st.spin[0] + st.spin[1]
+
+    def _event(self):
+        ev = self.torch.cuda.Event(enable_timing=True)
+        ev.record()
+        return ev
+
+    def _forces(self, guess):
+        """
+        (SCF state, dE/dR) at self.x from the device density ``guess``. With
+        ``phase_events`` a list, appends CUDA events (start, SCF done,
+        gradient done) of the call, for timing the two phases separately.
+        """
+        evs = self.phase_events
+        e0 = self._event() if evs is not None else None
+        if not self.autograd:
+            st = self._run(self.solver, self.x, guess)
+            e1 = self._event() if evs is not None else None
+            g = self._grad(st, self.thr, self.fp32_cutoff)
+        else:
+            from .autograd import scf_energy
+            x = self.torch.as_tensor(self.x).clone().requires_grad_(True)
+            holder: dict = {}
+            e = scf_energy(x, self.solver, guess, holder, gradient_screening=self.thr)
+            e1 = self._event() if evs is not None else None
+            (g,) = self.torch.autograd.grad(e, x)
+            st = holder["state"]
+        if evs is not None:
+            evs.append((e0, e1, self._event()))
+        return st, g
 
     def step(self):
         dt = self.dt
@@ -178,8 +212,7 @@ class DeviceXLBOMD:
             diss = diss + ck * pk
         guess = 2.0 * h[0] - h[1] + self.kappa * (D - h[0]) + self.alpha * diss
         self.history = [guess] + h[:-1]
-        self.state = self._run(self.solver, self.x, guess)
-        self.gradient = self._grad(self.state, self.thr, self.fp32_cutoff)
+        self.state, self.gradient = self._forces(guess)
         acc = -self.gradient.cpu().numpy() / self.m[:, None]
         self.v += 0.5 * dt * acc
         if self.thermo is not None:

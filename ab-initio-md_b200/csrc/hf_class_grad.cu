@@ -29,10 +29,12 @@ using RT = float;
 #define AIMD_GRAD_NAME AIMD_CAT(AIMD_CAT(AIMD_CAT(launch_grad32_c, AIMD_CLASS), _), AIMD_KET)
 #endif
 
-cudaError_t AIMD_GRAD_NAME(const LaunchEnv& e, const GradArgs& a, cudaStream_t st) {
+cudaError_t AIMD_GRAD_NAME(const LaunchEnv& e, const GradArgs& a0, cudaStream_t st) {
     const int cnt = e.cls_count[CX];
     if (cnt == 0 || e.cls_count[CY] == 0) return cudaSuccess;
-    const size_t smem = grad_smem_bytes<CX, RT>(e.natm, e.maxbp[CX]);
+    GradArgs a = a0;
+    a.rbuf = grad_rbuf_elems<CX, CY, RT>(e.maxbp[CX], e.maxbp[CY]);
+    const size_t smem = grad_smem_bytes<CX, RT>(e.natm, e.maxbp[CX], a.rbuf);
     cudaError_t r = set_smem_limit((const void*)grad2e_bra_kernel<CX, CY, RT>, smem);
     if (r != cudaSuccess) return r;
     grad2e_bra_kernel<CX, CY, RT><<<cnt, 128, smem, st>>>(a);

@@ -35,7 +35,16 @@ using RT = float;
 #endif
 
 template <int YK>
-cudaError_t launch_one(const LaunchEnv& e, const JKArgs& a, cudaStream_t st, size_t smem) {
+cudaError_t launch_one(const LaunchEnv& e, const JKArgs& a0, cudaStream_t st) {
+    JKArgs a = a0;
+    a.rbuf = jk_rbuf_elems<CX, YK, RT>(e.maxbp[CX], YK >= 0 ? e.maxbp[YK] : 1);
+    // K rows in shared memory unless they would not fit (large bases) or
+    // the context asks for global rows
+    size_t smem = jk_smem_bytes<CX, 1, RT>(e.nao, e.maxbp[CX], a.rbuf, a.kglobal != 0);
+    if (!a.kglobal && smem + static_smem((const void*)jk_bra_kernel<CX, 1, RT, YK>) > kSmemLimit) {
+        a.kglobal = 1;
+        smem = jk_smem_bytes<CX, 1, RT>(e.nao, e.maxbp[CX], a.rbuf, true);
+    }
     cudaError_t r = set_smem_limit((const void*)jk_bra_kernel<CX, 1, RT, YK>, smem);
     if (r != cudaSuccess) return r;
     jk_bra_kernel<CX, 1, RT, YK><<<e.cls_count[CX], JK_THREADS, smem, st>>>(a);
@@ -47,17 +56,16 @@ cudaError_t launch_one(const LaunchEnv& e, const JKArgs& a, cudaStream_t st, siz
 cudaError_t AIMD_JK_NAME(const LaunchEnv& e, const JKArgs& a, cudaStream_t st) {
     const int cnt = e.cls_count[CX];
     if (cnt == 0) return cudaSuccess;
-    const size_t smem = jk_smem_bytes<CX, 1, RT>(e.nao, e.maxbp[CX]);
     if constexpr (!JKKernel<CX, 1>::SPLIT) {
-        return launch_one<-1>(e, a, st, smem);
+        return launch_one<-1>(e, a, st);
     } else {
         cudaError_t r = cudaSuccess;
-        if constexpr (CX >= 5) if (r == cudaSuccess && e.cls_count[5]) r = launch_one<5>(e, a, st, smem);
-        if constexpr (CX >= 4) if (r == cudaSuccess && e.cls_count[4]) r = launch_one<4>(e, a, st, smem);
-        if (r == cudaSuccess && e.cls_count[3]) r = launch_one<3>(e, a, st, smem);
-        if (r == cudaSuccess && e.cls_count[2]) r = launch_one<2>(e, a, st, smem);
-        if (r == cudaSuccess && e.cls_count[1]) r = launch_one<1>(e, a, st, smem);
-        if (r == cudaSuccess && e.cls_count[0]) r = launch_one<0>(e, a, st, smem);
+        if constexpr (CX >= 5) if (r == cudaSuccess && e.cls_count[5]) r = launch_one<5>(e, a, st);
+        if constexpr (CX >= 4) if (r == cudaSuccess && e.cls_count[4]) r = launch_one<4>(e, a, st);
+        if constexpr (CX >= 3) if (r == cudaSuccess && e.cls_count[3]) r = launch_one<3>(e, a, st);
+        if constexpr (CX >= 2) if (r == cudaSuccess && e.cls_count[2]) r = launch_one<2>(e, a, st);
+        if (r == cudaSuccess && e.cls_count[1]) r = launch_one<1>(e, a, st);
+        if (r == cudaSuccess && e.cls_count[0]) r = launch_one<0>(e, a, st);
         return r;
     }
 }

@@ -180,15 +180,19 @@ __device__ __forceinline__ void boys_scaled(float alpha, float T, float (&g)[L +
     }
 }
 
-// R_tuv(alpha, PQ) for all t+u+v <= L, in place: levels n = L..0, each level
-// overwriting the previous one in decreasing Hermite index (entries h only
-// read lower indices of the level above). R[0] of level n is (-2a)^n F_n.
+// scale * R_tuv(alpha, PQ) for all t+u+v <= L, in place: levels n = L..0,
+// each level overwriting the previous one in decreasing Hermite index
+// (entries h only read lower indices of the level above). R[0] of level n
+// is scale (-2a)^n F_n; the recursion is linear in these seeds. R is a
+// register array or a pointer (shared memory) with NH(L) entries.
 // RT = double (plain path) or float (mixed-precision quartets).
-template <int L, typename RT>
-__device__ __forceinline__ void hermite_r(RT alpha, RT X, RT Y, RT Z, RT (&R)[nherm(L)]) {
+template <int L, typename RT, typename Arr>
+__device__ __forceinline__ void hermite_r_scaled(RT alpha, RT X, RT Y, RT Z, RT scale, Arr&& R) {
     const RT T = alpha * (X * X + Y * Y + Z * Z);
     RT g[L + 1];
     boys_scaled<L>(alpha, T, g);
+#pragma unroll
+    for (int n = 0; n <= L; ++n) g[n] *= scale;
     R[0] = g[L];
 #pragma unroll
     for (int n = L - 1; n >= 0; --n) {
@@ -217,6 +221,11 @@ __device__ __forceinline__ void hermite_r(RT alpha, RT X, RT Y, RT Z, RT (&R)[nh
         }
         R[0] = g[n];
     }
+}
+
+template <int L, typename RT>
+__device__ __forceinline__ void hermite_r(RT alpha, RT X, RT Y, RT Z, RT (&R)[nherm(L)]) {
+    hermite_r_scaled<L>(alpha, X, Y, Z, RT(1), R);
 }
 
 // E^{ij}_t for i <= IM, j <= JM, t <= i + j, one direction: e[i][j][t].
@@ -256,7 +265,10 @@ __device__ __forceinline__ void hermite_e(RT pa, RT pb, RT oo2p, RT e00, RT (&e)
 
 // Primitive-pair record (PPW doubles), pair oriented so that l_A >= l_B:
 //   0 a, 1 b, 2 K = exp(-mu |A-B|^2), 3..5 P, 6..8 P - A, 9..11 P - B,
-//   12..15 contraction products c_A[ca] c_B[cb] at index ca * ncon_B + cb
+//   12..15 contraction products c_A[ca] c_B[cb] at the compact index
+//          ca * nB + cb (nA, nB: the blocks' actual contraction counts),
+//          zeros after nA * nB; the bra rows and ket contraction groups of
+//          the quartet kernels use the same compact index
 struct PairView {
     const int* pa_blk;      // [npair] block A (l_A >= l_B)
     const int* pb_blk;      // [npair] block B

@@ -21,6 +21,9 @@
 
 namespace hf {
 
+#ifndef AIMD_RSMEM_MINL
+#define AIMD_RSMEM_MINL 4
+#endif
 template <int CX, int CY>
 struct QClass {
     static constexpr int LA = cls_la(CX), LB = cls_lb(CX), LC = cls_la(CY), LD = cls_lb(CY);
@@ -35,6 +38,10 @@ struct QClass {
     static constexpr int KG = NROW * KCD <= 24 ? KCD : ((KCD % 2 == 0 && NROW * 2 <= 24) ? 2 : 1);
     static constexpr int NKG = KCD / KG;
     static constexpr int NHB = nherm(LAB);
+    // R_tuv staged once per primitive quartet for all columns of a ket pair
+    // (two-stage items) when the ket pair has several columns and R is not
+    // trivially cheap
+    static constexpr bool RSMEM = CY >= 1 && L >= AIMD_RSMEM_MINL;
 };
 
 // Bra-side E tables with an extra +G in i and j (G = 1 for gradients).
@@ -128,12 +135,23 @@ __device__ __forceinline__ void select_row(const RT (&e)[IM + 1][JM + 1][T + 1],
 }
 
 // v[r][kk] = (row r | cd, contraction kk) of the quartet (staged bra pair,
-// ket pair records rk with nkp primitive pairs); r = (ka*KB + kb)*NAB +
-// ia*NB + jb, kk = kc*KD + kd. Ket primitives outermost (each record is read
-// once), bra primitives inner (shared-memory broadcast).
-template <int CX, int CY, typename RT>
+// ket pair records rk with nkp primitive pairs); r = (ka*nB + kb)*NAB +
+// ia*NB + jb, kk = kc*nD + kd - kg*KG (compact contraction indices over the
+// blocks' actual counts).
+// Loop order: bra primitives outer; for each, the ket primitives inner,
+// where the ket step X_tuv (bra Hermite index tuv) of every primitive
+// quartet is summed with its ket contraction coefficients,
+// Xs[kk]_tuv = sum_ik c_ik[kk] X_tuv(ib, ik); the bra Hermite->Cartesian
+// step, linear in X, then runs once per bra primitive instead of once per
+// primitive quartet (the reference applies it per primitive quartet,
+// aimd/qc/integrals.py:777-842).
+// RS = false: R_tuv of each primitive quartet is computed here; RS = true:
+// it is read from Rs, [ik][ib][NH(L)] pref * R_tuv staged by the CTA
+// (stage_r below) once for all the columns of the ket pair.
+template <int CX, int CY, typename RT, bool RS = false>
 __device__ __forceinline__ void eri_column(const BraStageT<RT>& st, const double* __restrict__ rk, int nkp, int ic,
-                                           int id, int kg, RT (&v)[QClass<CX, CY>::NROW][QClass<CX, CY>::KG]) {
+                                           int id, int kg, RT (&v)[QClass<CX, CY>::NROW][QClass<CX, CY>::KG],
+                                           const RT* __restrict__ Rs = nullptr) {
     using Q = QClass<CX, CY>;
     using BE = BraE<Q::LA, Q::LB, 0>;
     constexpr int LA = Q::LA, LB = Q::LB, LC = Q::LC, LD = Q::LD, LAB = Q::LAB, LCD = Q::LCD, L = Q::L;
@@ -146,87 +164,109 @@ __device__ __forceinline__ void eri_column(const BraStageT<RT>& st, const double
     for (int r = 0; r < Q::NROW; ++r)
 #pragma unroll
         for (int k = 0; k < Q::KG; ++k) v[r][k] = RT(0);
-    for (int ik = 0; ik < nkp; ++ik) {
-        const KetRecT<RT> k = load_ket<RT>(rk + (size_t)ik * PPW);
-        const RT q = k.a + k.b, oo2q = RT(0.5) / q, iq = RT(2) * oo2q;
-        // ket E coefficients of this column only (box t2 <= cx+dx, ...)
-        RT ex[LCD + 1], ey[LCD + 1], ez[LCD + 1];
-        {
-            RT e[LC + 1][LD + 1][LCD + 1];
-            hermite_e<LC, LD>(k.QAx, k.QBx, oo2q, k.K, e);
-            select_row<LC, LD, LCD>(e, cx, dx, ex);
-            hermite_e<LC, LD>(k.QAy, k.QBy, oo2q, RT(1), e);
-            select_row<LC, LD, LCD>(e, cy, dy, ey);
-            hermite_e<LC, LD>(k.QAz, k.QBz, oo2q, RT(1), e);
-            select_row<LC, LD, LCD>(e, cz, dz, ez);
-        }
-        RT ck[Q::KG];
+    for (int ib = 0; ib < st.nbp; ++ib) {
+        const RT* sb = st.SB + ib * SBW;
+        RT Xs[Q::KG][Q::NHB];
 #pragma unroll
-        for (int i = 0; i < Q::KG; ++i) {
-            RT c = k.c[0];
+        for (int k = 0; k < Q::KG; ++k)
 #pragma unroll
-            for (int j = 1; j < Q::KCD; ++j)
-                if (j == kg * Q::KG + i) c = k.c[j];
-            ck[i] = c * fcd;
-        }
-        for (int ib = 0; ib < st.nbp; ++ib) {
-            const RT* sb = st.SB + ib * SBW;
-            const RT p = sb[0];
-            const RT rs = rsqrt_t(p + q);
-            const RT alpha = p * q * rs * rs;
-            const RT pref = RT(TWO_PI_2_5) * sb[1] * iq * rs;
-            RT R[nherm(L)];
-            hermite_r<L>(alpha, sb[2] - k.Qx, sb[3] - k.Qy, sb[4] - k.Qz, R);
-            RT X[Q::NHB];
+            for (int h = 0; h < Q::NHB; ++h) Xs[k][h] = RT(0);
+        for (int ik = 0; ik < nkp; ++ik) {
+            const KetRecT<RT> k = load_ket<RT>(rk + (size_t)ik * PPW);
+            const RT q = k.a + k.b, oo2q = RT(0.5) / q;
+            // ket E coefficients of this column only (box t2 <= cx+dx, ...)
+            RT ex[LCD + 1], ey[LCD + 1], ez[LCD + 1];
+            {
+                RT e[LC + 1][LD + 1][LCD + 1];
+                hermite_e<LC, LD>(k.QAx, k.QBx, oo2q, k.K, e);
+                select_row<LC, LD, LCD>(e, cx, dx, ex);
+                hermite_e<LC, LD>(k.QAy, k.QBy, oo2q, RT(1), e);
+                select_row<LC, LD, LCD>(e, cy, dy, ey);
+                hermite_e<LC, LD>(k.QAz, k.QBz, oo2q, RT(1), e);
+                select_row<LC, LD, LCD>(e, cz, dz, ez);
+            }
+            RT ck[Q::KG];
+#pragma unroll
+            for (int i = 0; i < Q::KG; ++i) {
+                RT c = k.c[0];
+#pragma unroll
+                for (int j = 1; j < Q::KCD; ++j)
+                    if (j == kg * Q::KG + i) c = k.c[j];
+                ck[i] = c * fcd;
+            }
+            // ket step: Xs[kk]_tuv += ck[kk] pref sum_{box(cd)} (-1)^|k| E^{cd}_k R_{tuv+k}
+            auto ket_step = [&](const auto& R, RT scale) {
+                RT sc[Q::KG];
+#pragma unroll
+                for (int kk = 0; kk < Q::KG; ++kk) sc[kk] = scale * ck[kk];
 #pragma unroll UH
-            for (int t = 0; t <= LAB; ++t)
+                for (int t = 0; t <= LAB; ++t)
 #pragma unroll UH
-                for (int u = 0; u <= LAB - t; ++u)
+                    for (int u = 0; u <= LAB - t; ++u)
 #pragma unroll
-                    for (int w = 0; w <= LAB - t - u; ++w) {
-                        RT s = RT(0);
+                        for (int w = 0; w <= LAB - t - u; ++w) {
+                            RT s = RT(0);
 #pragma unroll
-                        for (int t2 = 0; t2 <= LCD; ++t2) {
-                            if (t2 > cx + dx) continue;
+                            for (int t2 = 0; t2 <= LCD; ++t2) {
+                                if (t2 > cx + dx) continue;
 #pragma unroll
-                            for (int u2 = 0; u2 <= LCD; ++u2) {
-                                if (u2 > cy + dy) continue;
-                                const RT exy = ((t2 + u2) & 1) ? -ex[t2] * ey[u2] : ex[t2] * ey[u2];
+                                for (int u2 = 0; u2 <= LCD; ++u2) {
+                                    if (u2 > cy + dy) continue;
+                                    const RT exy = ((t2 + u2) & 1) ? -ex[t2] * ey[u2] : ex[t2] * ey[u2];
 #pragma unroll
-                                for (int v2 = 0; v2 <= LCD; ++v2) {
-                                    if (v2 > cz + dz) continue;
-                                    const RT e = (v2 & 1) ? -exy * ez[v2] : exy * ez[v2];
-                                    s += e * R[hidx(t + t2, u + u2, w + v2)];
+                                    for (int v2 = 0; v2 <= LCD; ++v2) {
+                                        if (v2 > cz + dz) continue;
+                                        const RT e = (v2 & 1) ? -exy * ez[v2] : exy * ez[v2];
+                                        s += e * R[hidx(t + t2, u + u2, w + v2)];
+                                    }
                                 }
                             }
+#pragma unroll
+                            for (int kk = 0; kk < Q::KG; ++kk) Xs[kk][hidx(t, u, w)] += sc[kk] * s;
                         }
-                        X[hidx(t, u, w)] = pref * s;
-                    }
-            // bra step: v[(ka,kb),ab][kk] += C[ka,kb] f_ab sum_box E^{ab}_tuv X[tuv] ck[kk]
-            const RT* E = st.E + (size_t)ib * BE::SIZE;
+            };
+            if constexpr (RS) {
+                ket_step(Rs + (size_t)(ik * st.nbp + ib) * nherm(L), RT(1));
+            } else {
+                const RT p = sb[0];
+                const RT rs = rsqrt_t(p + q);
+                const RT alpha = p * q * rs * rs;
+                const RT pref = RT(TWO_PI_2_5) * sb[1] * (RT(2) * oo2q) * rs;
+                RT R[nherm(L)];
+                hermite_r<L>(alpha, sb[2] - k.Qx, sb[3] - k.Qy, sb[4] - k.Qz, R);
+                ket_step(R, pref);
+            }
+        }
+        // bra step, once per bra primitive:
+        // v[(ka,kb),ab][kk] += C[ka,kb] f_ab sum_box E^{ab}_tuv Xs[kk]_tuv
+        const RT* E = st.E + (size_t)ib * BE::SIZE;
 #pragma unroll UH
-            for (int ia = 0; ia < Q::NA; ++ia) {
-                const int ax = cart_x(LA, ia), ay = cart_y(LA, ia), az = cart_z(LA, ia);
+        for (int ia = 0; ia < Q::NA; ++ia) {
+            const int ax = cart_x(LA, ia), ay = cart_y(LA, ia), az = cart_z(LA, ia);
 #pragma unroll
-                for (int jb = 0; jb < Q::NB; ++jb) {
-                    const int bx = cart_x(LB, jb), by = cart_y(LB, jb), bz = cart_z(LB, jb);
-                    const RT fab = static_cast<RT>(cart_norm(ax, ay, az) * cart_norm(bx, by, bz));
-                    RT s = RT(0);
+            for (int jb = 0; jb < Q::NB; ++jb) {
+                const int bx = cart_x(LB, jb), by = cart_y(LB, jb), bz = cart_z(LB, jb);
+                const RT fab = static_cast<RT>(cart_norm(ax, ay, az) * cart_norm(bx, by, bz));
+                RT s[Q::KG];
 #pragma unroll
-                    for (int t = 0; t <= ax + bx; ++t)
+                for (int kk = 0; kk < Q::KG; ++kk) s[kk] = RT(0);
 #pragma unroll
-                        for (int u = 0; u <= ay + by; ++u) {
-                            const RT exy = E[BE::at(0, ax, bx, t)] * E[BE::at(1, ay, by, u)];
+                for (int t = 0; t <= ax + bx; ++t)
 #pragma unroll
-                            for (int w = 0; w <= az + bz; ++w) s += exy * E[BE::at(2, az, bz, w)] * X[hidx(t, u, w)];
+                    for (int u = 0; u <= ay + by; ++u) {
+                        const RT exy = E[BE::at(0, ax, bx, t)] * E[BE::at(1, ay, by, u)];
+#pragma unroll
+                        for (int w = 0; w <= az + bz; ++w) {
+                            const RT e = exy * E[BE::at(2, az, bz, w)];
+#pragma unroll
+                            for (int kk = 0; kk < Q::KG; ++kk) s[kk] += e * Xs[kk][hidx(t, u, w)];
                         }
-                    s *= fab;
-#pragma unroll
-                    for (int kab = 0; kab < Q::KAB; ++kab) {
-                        const RT c = sb[8 + kab] * s;
-#pragma unroll
-                        for (int kk = 0; kk < Q::KG; ++kk) v[kab * Q::NAB + ia * Q::NB + jb][kk] += c * ck[kk];
                     }
+#pragma unroll
+                for (int kab = 0; kab < Q::KAB; ++kab) {
+                    const RT c = sb[8 + kab] * fab;
+#pragma unroll
+                    for (int kk = 0; kk < Q::KG; ++kk) v[kab * Q::NAB + ia * Q::NB + jb][kk] += c * s[kk];
                 }
             }
         }
@@ -294,6 +334,10 @@ struct JKArgs {
     const double* bmax; // [nblock][nblock] max |D| per block pair (all sets)
     int nblock;
     double dthr;
+    size_t rbuf;        // elements of the kernel's staged-R buffer (set per launch)
+    // 1: the K rows of the bra functions accumulate in global memory (set per
+    // launch when the per-CTA shared rows, NF x nao doubles, would not fit)
+    int kglobal;
 };
 
 // Digest one column (fixed ket component pair cd, all ket contractions kk)
@@ -323,12 +367,14 @@ __device__ __forceinline__ void jk_digest_column(const JKArgs& a, const ST& st, 
         const double* __restrict__ D = a.D + s * nn;
         // K rows of the bra functions: shared accumulator, or the global K
         // itself (KGLOBAL, for bra classes whose rows would not fit)
-        double* Ks = KGLOBAL ? nullptr : Ksm + (size_t)s * NF * n;
+        const bool kgl = KGLOBAL || a.kglobal;
+        double* Ks = kgl ? nullptr : Ksm + (size_t)s * NF * n;
         double* Kg = a.K + s * nn;
 #pragma unroll
         for (int kk = 0; kk < Q::KG; ++kk) {
-                const int kq = kg * Q::KG + kk, kc = kq / Q::KD, kd = kq % Q::KD;
-                if (kc >= nC || kd >= nD) continue;
+                const int kq = kg * Q::KG + kk;
+                if (kq >= nC * nD) continue;
+                const int kc = kq / nD, kd = kq % nD;
                 const int l = oC + kc * Q::NC + ic, sg = oD + kd * Q::ND + id;
                 const double dls = __ldg(D + (size_t)l * n + sg);
                 double jcd = 0.0;
@@ -341,7 +387,7 @@ __device__ __forceinline__ void jk_digest_column(const JKArgs& a, const ST& st, 
                         for (int ia = 0; ia < Q::NA; ++ia)
 #pragma unroll
                             for (int jb = 0; jb < Q::NB; ++jb) {
-                                const int r = (ka * Q::KB + kb) * Q::NAB + ia * Q::NB + jb;
+                                const int r = (ka * st.nB + kb) * Q::NAB + ia * Q::NB + jb;
                                 const int m = st.oA + ka * Q::NA + ia, nb_ = st.oB + kb * Q::NB + jb;
                                 jcd += v[r][kk] * __ldg(D + (size_t)m * n + nb_);
                                 Jt[(s * Q::NROW + r) * blockDim.x + threadIdx.x] += 2.0 * g * v[r][kk] * dls;
@@ -360,12 +406,12 @@ __device__ __forceinline__ void jk_digest_column(const JKArgs& a, const ST& st, 
 #pragma unroll
                             for (int jb = 0; jb < Q::NB; ++jb) {
                                 if (kb >= st.nB) continue;
-                                const int r = (ka * Q::KB + kb) * Q::NAB + ia * Q::NB + jb;
+                                const int r = (ka * st.nB + kb) * Q::NAB + ia * Q::NB + jb;
                                 const size_t nb_ = st.oB + kb * Q::NB + jb;
                                 s1 += v[r][kk] * __ldg(D + nb_ * n + sg);
                                 s2 += v[r][kk] * __ldg(D + nb_ * n + l);
                             }
-                        double* row = KGLOBAL ? Kg + (size_t)(st.oA + ka * Q::NA + ia) * n
+                        double* row = kgl ? Kg + (size_t)(st.oA + ka * Q::NA + ia) * n
                                               : Ks + (size_t)(ka * Q::NA + ia) * n;
                         atomicAdd(row + l, g * s1);
                         atomicAdd(row + sg, g * s2);
@@ -382,12 +428,12 @@ __device__ __forceinline__ void jk_digest_column(const JKArgs& a, const ST& st, 
 #pragma unroll
                             for (int ia = 0; ia < Q::NA; ++ia) {
                                 if (ka >= st.nA) continue;
-                                const int r = (ka * Q::KB + kb) * Q::NAB + ia * Q::NB + jb;
+                                const int r = (ka * st.nB + kb) * Q::NAB + ia * Q::NB + jb;
                                 const size_t m = st.oA + ka * Q::NA + ia;
                                 s1 += v[r][kk] * __ldg(D + m * n + sg);
                                 s2 += v[r][kk] * __ldg(D + m * n + l);
                             }
-                        double* row = KGLOBAL ? Kg + (size_t)(st.oB + kb * Q::NB + jb) * n
+                        double* row = kgl ? Kg + (size_t)(st.oB + kb * Q::NB + jb) * n
                                               : Ks + (size_t)(NFA + kb * Q::NB + jb) * n;
                         atomicAdd(row + l, g * s1);
                         atomicAdd(row + sg, g * s2);
@@ -404,13 +450,24 @@ __device__ __forceinline__ void jk_digest_column(const JKArgs& a, const ST& st, 
 // chunk ended (rot), so ragged tails do not pile up on the low threads.
 // Every thread of the CTA must call this with the same j0 and cnt.
 constexpr int KQ_CAP = 256;
+
+// Ket contraction groups of KG combinations that a segment's pairs need: its
+// pairs carry 1, 2 or 4 contraction combinations (sub-class contraction
+// bucket), stored first in the compact index, so groups past them are empty.
+template <int KG, int NKG>
+__device__ __forceinline__ int seg_groups(int sub) {
+    const int cb = sub % NCONB;
+    const int ncs = cb == 0 ? 1 : (cb == 1 ? 2 : 4);
+    const int g = (ncs + KG - 1) / KG;
+    return g < NKG ? g : NKG;
+}
 struct KetQueue {
     int pos[KQ_CAP];
     int n;
 };
 
-template <int NPER, typename Keep, typename Work>
-__device__ __forceinline__ void ket_items(int j0, int64_t cnt, KetQueue& q, int& rot, Keep keep, Work work) {
+template <typename Queue, typename Keep, typename Work>
+__device__ __forceinline__ void ket_items(int nper, int j0, int64_t cnt, Queue& q, int& rot, Keep keep, Work work) {
     const int lane = threadIdx.x & 31;
     for (int64_t base = 0; base < cnt; base += KQ_CAP) {
         const int m = static_cast<int>(cnt - base < KQ_CAP ? cnt - base : KQ_CAP);
@@ -427,7 +484,7 @@ __device__ __forceinline__ void ket_items(int j0, int64_t cnt, KetQueue& q, int&
             if (k) q.pos[w0 + __popc(mask & ((1u << lane) - 1u))] = pos;
         }
         __syncthreads();
-        const int items = q.n * NPER;
+        const int items = q.n * nper;
         int it = static_cast<int>(threadIdx.x) - rot;
         if (it < 0) it += blockDim.x;
         // column-major: neighbouring lanes take the same ket column of
@@ -439,9 +496,162 @@ __device__ __forceinline__ void ket_items(int j0, int64_t cnt, KetQueue& q, int&
     }
 }
 
+// ---- Two-stage items: R_tuv staged in shared memory
+// A ket pair of class Y carries NCD Cartesian columns (x contraction
+// groups), each one work item; R_tuv of a primitive quartet is the same for
+// all of them. For the classes where recomputing it per item costs (RSmem
+// below), each queue chunk is cut into sub-chunks whose primitive quartets
+// fit RB_PQ slots of a shared buffer (plus the largest single ket pair),
+// and per sub-chunk:
+//   stage 1: one thread per primitive quartet (ket pair i, ket primitive ik,
+//            bra primitive ib) writes pref * R_tuv into the buffer;
+//   stage 2: the column items of the sub-chunk's ket pairs read it.
+template <int L, typename RT>
+struct RSmem {
+    static constexpr int NH = nherm(L);
+    // slots per sub-chunk: about 32 KB of R (FP64; 16 KB of FP32 R)
+    static constexpr int RB_PQ = (4096 + NH - 1) / NH;
+    // R level recursion in shared memory instead of registers from this L on
+    // (it would hold NH(L) values in registers for the whole kernel)
+    static constexpr bool INPLACE = L >= 6;
+};
+template <int L, typename RT>
+__host__ __device__ constexpr size_t rsmem_bytes(int max_bra_prims, int max_ket_prims) {
+    return sizeof(RT) * (size_t)nherm(L) * (RSmem<L, RT>::RB_PQ + (size_t)max_bra_prims * max_ket_prims);
+}
+
+struct KetQueueR {
+    int pos[KQ_CAP];
+    int pq[KQ_CAP + 1];     // exclusive prefix of primitive quartets over the chunk's entries
+    int sc[KQ_CAP];         // sub-chunk of each entry
+    int n;
+};
+
+// first index in [lo, hi) with a[i] >= key (a non-decreasing)
+__device__ __forceinline__ int lower_bound_i(const int* a, int lo, int hi, int key) {
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (a[mid] < key) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+// pref * R_tuv of primitive quartet (bra primitive ib of the stage, ket
+// primitive record kr) into out[NH(L)] (shared memory).
+template <int L, typename RT>
+__device__ __forceinline__ void stage_r(const BraStageT<RT>& st, int ib, const double* __restrict__ kr, RT* out) {
+    const double2* r2 = reinterpret_cast<const double2*>(kr);
+    const double2 ab = __ldg(r2 + 0), kq = __ldg(r2 + 1), qyz = __ldg(r2 + 2);
+    const RT* sb = st.SB + ib * SBW;
+    const RT p = sb[0], q = static_cast<RT>(ab.x) + static_cast<RT>(ab.y);
+    const RT rs = rsqrt_t(p + q);
+    const RT alpha = p * q * rs * rs;
+    const RT pref = RT(TWO_PI_2_5) * sb[1] * (RT(1) / q) * rs;
+    const RT X = sb[2] - static_cast<RT>(kq.y), Y = sb[3] - static_cast<RT>(qyz.x), Z = sb[4] - static_cast<RT>(qyz.y);
+    if constexpr (RSmem<L, RT>::INPLACE) {
+        hermite_r_scaled<L>(alpha, X, Y, Z, pref, out);
+    } else {
+        RT R[nherm(L)];
+        hermite_r_scaled<L>(alpha, X, Y, Z, pref, R);
+#pragma unroll
+        for (int h = 0; h < nherm(L); ++h) out[h] = R[h];
+    }
+}
+
+// ket_items with R staged per sub-chunk; work(pos, r, Rs) receives the ket
+// pair's staged R ([ik][ib][NH(L)]). Rbuf holds rsmem_bytes(...) bytes.
+template <int L, typename RT, typename Keep, typename Work>
+__device__ __forceinline__ void ket_items_r(int nper, int j0, int64_t cnt, KetQueueR& q, int& rot,
+                                            const BraStageT<RT>& st, const QuartetArgs& qa, RT* Rbuf, Keep keep,
+                                            Work work) {
+    constexpr int NH = nherm(L);
+    constexpr int B = RSmem<L, RT>::RB_PQ;
+    const int lane = threadIdx.x & 31;
+    const int nbp = st.nbp;
+    for (int64_t base = 0; base < cnt; base += KQ_CAP) {
+        const int m = static_cast<int>(cnt - base < KQ_CAP ? cnt - base : KQ_CAP);
+        if (threadIdx.x == 0) q.n = 0;
+        __syncthreads();
+        for (int i0 = 0; i0 < m; i0 += blockDim.x) {
+            const int i = i0 + threadIdx.x;
+            const int pos = j0 + static_cast<int>(base) + i;
+            const bool k = i < m && keep(pos);
+            const unsigned mask = __ballot_sync(0xffffffffu, k);
+            int w0 = 0;
+            if (lane == 0 && mask) w0 = atomicAdd(&q.n, __popc(mask));
+            w0 = __shfl_sync(0xffffffffu, w0, 0);
+            if (k) {
+                const int slot = w0 + __popc(mask & ((1u << lane) - 1u));
+                q.pos[slot] = pos;
+                q.pq[slot] = qa.pv.npp[qa.sorted[pos]] * nbp;      // primitive quartets of the entry
+            }
+        }
+        __syncthreads();
+        const int ne = q.n;
+        if (ne == 0) continue;                                      // uniform: q.n is shared
+        // warp 0: exclusive prefix of the entries' primitive quartets and
+        // their sub-chunks (an entry belongs to the sub-chunk of its last slot)
+        if (threadIdx.x < 32) {
+            constexpr int PER = KQ_CAP / 32;
+            int c[PER], local = 0;
+#pragma unroll
+            for (int k = 0; k < PER; ++k) {
+                const int i = lane * PER + k;
+                c[k] = i < ne ? q.pq[i] : 0;
+                local += c[k];
+            }
+            int incl = local;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, d);
+                if (lane >= d) incl += v;
+            }
+            __syncwarp();
+            int run = incl - local;
+#pragma unroll
+            for (int k = 0; k < PER; ++k) {
+                const int i = lane * PER + k;
+                if (i < ne) {
+                    q.pq[i] = run;
+                    q.sc[i] = (run + (c[k] > 0 ? c[k] : 1) - 1) / B;
+                    run += c[k];
+                }
+            }
+            if (lane == 31) q.pq[ne] = incl;
+        }
+        __syncthreads();
+        const int k0 = q.sc[0], k1 = q.sc[ne - 1];
+        for (int kc = k0; kc <= k1; ++kc) {
+            const int f = lower_bound_i(q.sc, 0, ne, kc), l = lower_bound_i(q.sc, f, ne, kc + 1);
+            if (f == l) continue;                                   // uniform across the CTA
+            const int pq0 = q.pq[f], npq = q.pq[l] - pq0;
+            // stage 1: R of every primitive quartet of the sub-chunk
+            for (int w = threadIdx.x; w < npq; w += blockDim.x) {
+                const int i = lower_bound_i(q.pq, f, l + 1, pq0 + w + 1) - 1;   // last entry with pq <= pq0 + w
+                const int rem = pq0 + w - q.pq[i];
+                const int ik = rem / nbp, ib = rem - ik * nbp;
+                const int P2 = qa.sorted[q.pos[i]];
+                stage_r<L>(st, ib, qa.pv.rec + (qa.pv.slot[P2] + ik) * PPW, Rbuf + (size_t)w * NH);
+            }
+            __syncthreads();
+            // stage 2: the column items of the sub-chunk, column-major as in ket_items
+            const int nsc = l - f;
+            const int items = nsc * nper;
+            int it = static_cast<int>(threadIdx.x) - rot;
+            if (it < 0) it += blockDim.x;
+            for (; it < items; it += blockDim.x) {
+                const int i = f + it % nsc;
+                work(q.pos[i], it / nsc, Rbuf + (size_t)(q.pq[i] - pq0) * NH);
+            }
+            rot = (rot + items) % static_cast<int>(blockDim.x);
+            __syncthreads();
+        }
+    }
+}
+
 template <int CX, int CY, int NS, bool KGLOBAL, typename RT>
 __device__ __forceinline__ void jk_ket_class(const JKArgs& a, const BraStageT<RT>& st, int spos, double* Jt,
-                                             double* Ksm, KetQueue& kq, int& rot) {
+                                             double* Ksm, KetQueueR& kq, int& rot, RT* Rbuf) {
     using Q = QClass<CX, CY>;
     const double q1 = a.q.sortedQ[spos];
     const double* bm = a.bmax;
@@ -461,13 +671,16 @@ __device__ __forceinline__ void jk_ket_class(const JKArgs& a, const BraStageT<RT
                                         fmax(bm[st.B * nb + C], bm[st.B * nb + Dd])));
             return q1 * a.q.sortedQ[pos] * dm >= a.dthr;
         };
-        auto work = [&](int pos, int r) {
-            const int kg = r % Q::NKG, cd = r / Q::NKG;
+        // contraction groups that the segment's ket pairs actually carry
+        const int nkg = seg_groups<Q::KG, Q::NKG>(sub);
+        auto work = [&](int pos, int r, const RT* Rs) {
+            const int kg = r % nkg, cd = r / nkg;
             const int P2 = a.q.sorted[pos];
             const int C = a.q.pv.pa_blk[P2], Dd = a.q.pv.pb_blk[P2];
             const int ic = cd / Q::ND, id = cd % Q::ND;
             RT v[Q::NROW][Q::KG];
-            eri_column<CX, CY>(st, a.q.pv.rec + a.q.pv.slot[P2] * PPW, a.q.pv.npp[P2], ic, id, kg, v);
+            eri_column<CX, CY, RT, Q::RSMEM>(st, a.q.pv.rec + a.q.pv.slot[P2] * PPW, a.q.pv.npp[P2], ic, id, kg, v,
+                                             Rs);
             if constexpr (sizeof(RT) == sizeof(double)) {
                 jk_digest_column<CX, CY, NS, KGLOBAL>(a, st, P2, C, Dd, ic, id, kg, v, Jt, Ksm);
             } else {
@@ -480,7 +693,13 @@ __device__ __forceinline__ void jk_ket_class(const JKArgs& a, const BraStageT<RT
                 jk_digest_column<CX, CY, NS, KGLOBAL>(a, st, P2, C, Dd, ic, id, kg, vd, Jt, Ksm);
             }
         };
-        ket_items<Q::NCD * Q::NKG>(a.q.seg_start[seg] + static_cast<int>(kb), ke - kb, kq, rot, keep, work);
+        const int j0 = a.q.seg_start[seg] + static_cast<int>(kb);
+        if constexpr (Q::RSMEM) {
+            ket_items_r<Q::L>(Q::NCD * nkg, j0, ke - kb, kq, rot, st, a.q, Rbuf, keep, work);
+        } else {
+            ket_items(Q::NCD * nkg, j0, ke - kb, kq, rot, keep,
+                      [&](int pos, int r) { work(pos, r, static_cast<const RT*>(nullptr)); });
+        }
     }
 }
 
@@ -516,14 +735,16 @@ __global__ void __launch_bounds__(JK_THREADS, AIMD_JK_MINB) jk_bra_kernel(JKArgs
     using Q0 = QClass<CX, 0>;
     extern __shared__ double smem[];
     const int n = a.q.nao;
+    const int krows = a.kglobal ? 0 : KK::KROWS;
     double* Ksm = smem;
-    double* Jt = Ksm + (size_t)KK::KROWS * n;
-    RT* Esm = reinterpret_cast<RT*>(Jt + NS * KK::NROW * JK_THREADS);
+    double* Jt = Ksm + (size_t)krows * n;
+    RT* Rbuf = reinterpret_cast<RT*>(Jt + NS * KK::NROW * JK_THREADS);
+    RT* Esm = Rbuf + a.rbuf;
     constexpr int yk = YK;
     const int spos = a.q.cls_start[CX] + (int)blockIdx.x;
     const int P1 = a.q.sorted[spos];
     __shared__ BraStageT<RT> st;
-    __shared__ KetQueue kq;
+    __shared__ KetQueueR kq;
     __shared__ int any;
     if (threadIdx.x == 0) {
         load_stage(a.q, P1, st, Esm);
@@ -539,17 +760,17 @@ __global__ void __launch_bounds__(JK_THREADS, AIMD_JK_MINB) jk_bra_kernel(JKArgs
     }
     __syncthreads();
     if (!any) return;
-    for (int i = threadIdx.x; i < KK::KROWS * n + NS * KK::NROW * JK_THREADS; i += blockDim.x) smem[i] = 0.0;
+    for (int i = threadIdx.x; i < krows * n + NS * KK::NROW * JK_THREADS; i += blockDim.x) smem[i] = 0.0;
     stage_bra_e<Q0::LA, Q0::LB, 0>(st);
     __syncthreads();
     constexpr bool KG_ = KK::KGLOBAL;
     int rot = 0;
-    if constexpr (yk < 0 || yk == 0) jk_ket_class<CX, 0, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot);
-    if constexpr (CX >= 1 && (yk < 0 || yk == 1)) jk_ket_class<CX, 1, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot);
-    if constexpr (CX >= 2 && (yk < 0 || yk == 2)) jk_ket_class<CX, 2, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot);
-    if constexpr (CX >= 3 && (yk < 0 || yk == 3)) jk_ket_class<CX, 3, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot);
-    if constexpr (CX >= 4 && (yk < 0 || yk == 4)) jk_ket_class<CX, 4, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot);
-    if constexpr (CX >= 5 && (yk < 0 || yk == 5)) jk_ket_class<CX, 5, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot);
+    if constexpr (yk < 0 || yk == 0) jk_ket_class<CX, 0, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot, Rbuf);
+    if constexpr (CX >= 1 && (yk < 0 || yk == 1)) jk_ket_class<CX, 1, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot, Rbuf);
+    if constexpr (CX >= 2 && (yk < 0 || yk == 2)) jk_ket_class<CX, 2, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot, Rbuf);
+    if constexpr (CX >= 3 && (yk < 0 || yk == 3)) jk_ket_class<CX, 3, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot, Rbuf);
+    if constexpr (CX >= 4 && (yk < 0 || yk == 4)) jk_ket_class<CX, 4, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot, Rbuf);
+    if constexpr (CX >= 5 && (yk < 0 || yk == 5)) jk_ket_class<CX, 5, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot, Rbuf);
     __syncthreads();
     const size_t nn = (size_t)n * n;
     // flush J_ab: one thread per (set, row) sums the per-thread slots
@@ -559,14 +780,14 @@ __global__ void __launch_bounds__(JK_THREADS, AIMD_JK_MINB) jk_bra_kernel(JKArgs
         if (val == 0.0) continue;
         const int s = i / KK::NROW, r = i % KK::NROW;
         const int kab = r / Q0::NAB, ab = r % Q0::NAB;
-        const int ka = kab / Q0::KB, kb = kab % Q0::KB;
+        const int ka = kab / st.nB, kb = kab % st.nB;
         const int m = st.oA + ka * Q0::NA + ab / Q0::NB, nb_ = st.oB + kb * Q0::NB + ab % Q0::NB;
         atomicAdd(a.J + s * nn + (size_t)m * n + nb_, val);
     }
     // flush K rows
-    if constexpr (!KK::KGLOBAL) {
+    if (krows > 0) {
         constexpr int NFA = Q0::KA * Q0::NA;
-        for (int i = threadIdx.x; i < KK::KROWS * n; i += blockDim.x) {
+        for (int i = threadIdx.x; i < krows * n; i += blockDim.x) {
             const double val = Ksm[i];
             if (val == 0.0) continue;
             const int col = i % n, f = (i / n) % KK::NF, s = i / (n * KK::NF);
@@ -576,11 +797,22 @@ __global__ void __launch_bounds__(JK_THREADS, AIMD_JK_MINB) jk_bra_kernel(JKArgs
     }
 }
 
+// Elements of the staged-R buffer of the (CX, YK) kernel (0 unless two-stage).
+template <int CX, int YK, typename RT>
+size_t jk_rbuf_elems(int max_bra_prims, int max_ket_prims) {
+    if constexpr (YK >= 0) {
+        using Q = QClass<CX, YK>;
+        if constexpr (Q::RSMEM) return rsmem_bytes<Q::L, RT>(max_bra_prims, max_ket_prims) / sizeof(RT);
+    }
+    return 0;
+}
+
 template <int CX, int NS, typename RT>
-size_t jk_smem_bytes(int nao, int max_bra_prims) {
+size_t jk_smem_bytes(int nao, int max_bra_prims, size_t rbuf_elems, bool kglobal) {
     using KK = JKKernel<CX, NS>;
-    return sizeof(double) * ((size_t)KK::KROWS * nao + (size_t)NS * KK::NROW * JK_THREADS) +
-           sizeof(RT) * (size_t)max_bra_prims * (KK::ESIZE + SBW);
+    const size_t krows = kglobal ? 0 : KK::KROWS;
+    return sizeof(double) * (krows * nao + (size_t)NS * KK::NROW * JK_THREADS) +
+           sizeof(RT) * (rbuf_elems + (size_t)max_bra_prims * (KK::ESIZE + SBW));
 }
 
 // ---------------------------------------------------------- Schwarz
@@ -611,7 +843,7 @@ __global__ void __launch_bounds__(64) schwarz_kernel(QuartetArgs a, const int* p
 #pragma unroll
             for (int kb = 0; kb < Q::KB; ++kb) {
                 if (ka >= st.nA || kb >= st.nB) continue;
-                const int kk = ka * Q::KB + kb;
+                const int kk = ka * st.nB + kb;
 #pragma unroll
                 for (int r = 0; r < Q::NROW; ++r)
                     if (r == kk * Q::NAB + cd) m = fmax(m, fabs(v[r][kk]));

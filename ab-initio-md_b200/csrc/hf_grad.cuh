@@ -27,6 +27,7 @@ struct GradArgs {
     double thr;             // exact screening threshold on Q1 Q2 max|Gamma|
     double* grad;           // [natm][3]
     int natm;
+    size_t rbuf;            // elements of the kernel's staged-R buffer (set per launch)
     const double* bmc;      // [nblock][nblock] max |Dc| per block pair
     const double* bmx;      // [nblock][nblock] max over x of |Dx| per block pair (nx > 0)
     int nblock;
@@ -80,11 +81,224 @@ __device__ __forceinline__ void ket_deriv_rows(const RT (&e)[LC + 2][LD + 1][LC 
                 }
 }
 
-// Gradient contribution of one column; adds A, B parts to gab and C, D
-// parts to the shared accumulator gsh[natm][3].
+// Primitive loops of one gradient column with the bra-side work hoisted out
+// of the ket primitives: bra primitives outer; per bra primitive the
+// C-pass weights Y[kk]_h = sum_ab f_ab C_ab Gamma[ab][kk] E^{ab}_h (bra
+// only) are formed once, the ket primitives inner accumulate the ket step
+// Xs[kk]_h = sum_ik c_ik[kk] pref sum_box(cd) (-1)^|k| E^{cd}_k R_{h+k}
+// (h to LAB + 1) and the C pass, and the bra pass for centres A and B runs
+// once per bra primitive on Xs (it is linear in the ket step). Same sums as
+// the per-primitive-quartet order, regrouped.
+template <int CX, int CY, typename RT, bool RS>
+__device__ __forceinline__ void grad_prims_hoisted(const BraStageT<RT>& st, const RT (&Gr)[QClass<CX, CY>::NROW][QClass<CX, CY>::KG],
+                                                   const double* __restrict__ rk, int nkp, int ic, int id, int kg,
+                                                   RT (&dA)[3], RT (&dB)[3], RT (&dC)[3], const RT* __restrict__ Rs) {
+    using Q = QClass<CX, CY>;
+    using BE = BraE<Q::LA, Q::LB, 1>;
+    using BD = BraD<Q::LA, Q::LB>;
+    constexpr int LA = Q::LA, LB = Q::LB, LC = Q::LC, LD = Q::LD, LAB = Q::LAB, LCD = Q::LCD, L = Q::L + 1;
+    constexpr int NH1 = nherm(LAB + 1);
+    constexpr int KG = Q::KG;
+    constexpr int UH = L >= 5 ? 1 : 16;
+    constexpr int UW = L >= 7 ? 1 : 16;
+    const int cx = cart_x(LC, ic), cy = cart_y(LC, ic), cz = cart_z(LC, ic);
+    const int dx = cart_x(LD, id), dy = cart_y(LD, id), dz = cart_z(LD, id);
+    const RT fcd = cart_norm(cx, cy, cz) * cart_norm(dx, dy, dz);
+    for (int ib = 0; ib < st.nbp; ++ib) {
+        const RT* sb = st.SB + ib * SBW;
+        const RT* E = st.E + (size_t)ib * BE::SIZE;
+        const RT* Db = st.D + (size_t)ib * BD::SIZE;
+        // Gamma of row ab contracted with this bra primitive's coefficients and f_ab
+        auto gq = [&](int ia, int jb, int kk) {
+            const RT fab = cart_norm(cart_x(LA, ia), cart_y(LA, ia), cart_z(LA, ia)) *
+                           cart_norm(cart_x(LB, jb), cart_y(LB, jb), cart_z(LB, jb));
+            RT s = RT(0);
+#pragma unroll
+            for (int kab = 0; kab < Q::KAB; ++kab) s += sb[8 + kab] * Gr[kab * Q::NAB + ia * Q::NB + jb][kk];
+            return s * fab;
+        };
+        RT Y[KG][Q::NHB];
+#pragma unroll
+        for (int kk = 0; kk < KG; ++kk)
+#pragma unroll
+            for (int h = 0; h < Q::NHB; ++h) Y[kk][h] = RT(0);
+#pragma unroll UH
+        for (int ia = 0; ia < Q::NA; ++ia) {
+            const int ax = cart_x(LA, ia), ay = cart_y(LA, ia), az = cart_z(LA, ia);
+#pragma unroll
+            for (int jb = 0; jb < Q::NB; ++jb) {
+                const int bx = cart_x(LB, jb), by = cart_y(LB, jb), bz = cart_z(LB, jb);
+                RT g[KG];
+#pragma unroll
+                for (int kk = 0; kk < KG; ++kk) g[kk] = gq(ia, jb, kk);
+#pragma unroll
+                for (int t = 0; t <= ax + bx; ++t)
+#pragma unroll
+                    for (int u = 0; u <= ay + by; ++u) {
+                        const RT e01 = E[BE::at(0, ax, bx, t)] * E[BE::at(1, ay, by, u)];
+#pragma unroll
+                        for (int w = 0; w <= az + bz; ++w) {
+                            const RT e = e01 * E[BE::at(2, az, bz, w)];
+#pragma unroll
+                            for (int kk = 0; kk < KG; ++kk) Y[kk][hidx(t, u, w)] += g[kk] * e;
+                        }
+                    }
+            }
+        }
+        RT Xs[KG][NH1];
+#pragma unroll
+        for (int kk = 0; kk < KG; ++kk)
+#pragma unroll
+            for (int h = 0; h < NH1; ++h) Xs[kk][h] = RT(0);
+        for (int ik = 0; ik < nkp; ++ik) {
+            const KetRecT<RT> k = load_ket<RT>(rk + (size_t)ik * PPW);
+            const RT ec = k.a, q = ec + k.b, oo2q = RT(0.5) / q;
+            RT ex[LCD + 2], ey[LCD + 2], ez[LCD + 2], gx[LCD + 2], gy[LCD + 2], gz[LCD + 2];
+            {
+                RT e[LC + 2][LD + 1][LCD + 2];
+                hermite_e<LC + 1, LD>(k.QAx, k.QBx, oo2q, k.K, e);
+                ket_deriv_rows<LC, LD>(e, cx, dx, ec, ex, gx);
+                hermite_e<LC + 1, LD>(k.QAy, k.QBy, oo2q, RT(1), e);
+                ket_deriv_rows<LC, LD>(e, cy, dy, ec, ey, gy);
+                hermite_e<LC + 1, LD>(k.QAz, k.QBz, oo2q, RT(1), e);
+                ket_deriv_rows<LC, LD>(e, cz, dz, ec, ez, gz);
+            }
+            RT ck[KG];
+#pragma unroll
+            for (int i = 0; i < KG; ++i) {
+                RT c = k.c[0];
+#pragma unroll
+                for (int j = 1; j < Q::KCD; ++j)
+                    if (j == kg * KG + i) c = k.c[j];
+                ck[i] = c * fcd;
+            }
+            auto body = [&](const auto& R, RT scale) {
+                RT sc[KG];
+#pragma unroll
+                for (int kk = 0; kk < KG; ++kk) sc[kk] = scale * ck[kk];
+                // ket step for the bra pass, accumulated over the ket primitives
+#pragma unroll UH
+                for (int t = 0; t <= LAB + 1; ++t)
+#pragma unroll UH
+                    for (int u = 0; u <= LAB + 1 - t; ++u)
+#pragma unroll UW
+                        for (int w = 0; w <= LAB + 1 - t - u; ++w) {
+                            RT s = RT(0);
+#pragma unroll
+                            for (int t2 = 0; t2 <= LCD; ++t2) {
+                                if (t2 > cx + dx) continue;
+#pragma unroll
+                                for (int u2 = 0; u2 <= LCD; ++u2) {
+                                    if (u2 > cy + dy) continue;
+                                    const RT exy = ((t2 + u2) & 1) ? -ex[t2] * ey[u2] : ex[t2] * ey[u2];
+#pragma unroll
+                                    for (int v2 = 0; v2 <= LCD; ++v2) {
+                                        if (v2 > cz + dz) continue;
+                                        s += ((v2 & 1) ? -exy * ez[v2] : exy * ez[v2]) * R[hidx(t + t2, u + u2, w + v2)];
+                                    }
+                                }
+                            }
+#pragma unroll
+                            for (int kk = 0; kk < KG; ++kk) Xs[kk][hidx(t, u, w)] += sc[kk] * s;
+                        }
+                // C pass: dC_d += sum_h Y_h sum_k (-1)^|k| dE^{cd}_{d,k} R_{h+k}
+#pragma unroll UH
+                for (int t = 0; t <= LAB; ++t)
+#pragma unroll UH
+                    for (int u = 0; u <= LAB - t; ++u)
+#pragma unroll UW
+                        for (int w = 0; w <= LAB - t - u; ++w) {
+                            RT yv = RT(0);
+#pragma unroll
+                            for (int kk = 0; kk < KG; ++kk) yv += sc[kk] * Y[kk][hidx(t, u, w)];
+                            RT s0 = RT(0), s1 = RT(0), s2 = RT(0);
+#pragma unroll
+                            for (int t2 = 0; t2 <= LCD + 1; ++t2) {
+                                if (t2 > cx + dx + 1) continue;
+#pragma unroll
+                                for (int u2 = 0; u2 <= LCD + 1; ++u2) {
+                                    if (u2 > cy + dy + 1) continue;
+#pragma unroll
+                                    for (int v2 = 0; v2 <= LCD + 1; ++v2) {
+                                        if (v2 > cz + dz + 1) continue;
+                                        const int over = (t2 > cx + dx) + (u2 > cy + dy) + (v2 > cz + dz);
+                                        if (over > 1) continue;
+                                        const RT r = ((t2 + u2 + v2) & 1) ? -R[hidx(t + t2, u + u2, w + v2)]
+                                                                              : R[hidx(t + t2, u + u2, w + v2)];
+                                        s0 += gx[t2] * ey[u2] * ez[v2] * r;
+                                        s1 += ex[t2] * gy[u2] * ez[v2] * r;
+                                        s2 += ex[t2] * ey[u2] * gz[v2] * r;
+                                    }
+                                }
+                            }
+                            dC[0] += yv * s0;
+                            dC[1] += yv * s1;
+                            dC[2] += yv * s2;
+                        }
+            };
+            if constexpr (RS) {
+                body(Rs + (size_t)(ik * st.nbp + ib) * nherm(L), RT(1));
+            } else {
+                const RT p = sb[0];
+                const RT rs = rsqrt_t(p + q);
+                const RT alpha = p * q * rs * rs;
+                const RT pref = RT(TWO_PI_2_5) * sb[1] * (RT(2) * oo2q) * rs;
+                RT R[nherm(L)];
+                hermite_r<L>(alpha, sb[2] - k.Qx, sb[3] - k.Qy, sb[4] - k.Qz, R);
+                body(R, pref);
+            }
+        }
+        // bra pass (A, B) on the summed ket step, once per bra primitive
+#pragma unroll UH
+        for (int ia = 0; ia < Q::NA; ++ia) {
+            const int ax = cart_x(LA, ia), ay = cart_y(LA, ia), az = cart_z(LA, ia);
+#pragma unroll
+            for (int jb = 0; jb < Q::NB; ++jb) {
+                const int bx = cart_x(LB, jb), by = cart_y(LB, jb), bz = cart_z(LB, jb);
+                RT g[KG];
+#pragma unroll
+                for (int kk = 0; kk < KG; ++kk) g[kk] = gq(ia, jb, kk);
+#pragma unroll
+                for (int t = 0; t <= ax + bx + 1; ++t)
+#pragma unroll
+                    for (int u = 0; u <= ay + by + 1; ++u)
+#pragma unroll
+                        for (int w = 0; w <= az + bz + 1; ++w) {
+                            const int over = (t > ax + bx) + (u > ay + by) + (w > az + bz);
+                            if (over > 1) continue;
+                            RT yv = RT(0);
+#pragma unroll
+                            for (int kk = 0; kk < KG; ++kk) yv += g[kk] * Xs[kk][hidx(t, u, w)];
+                            const RT e0 = E[BE::at(0, ax, bx, t)], e1 = E[BE::at(1, ay, by, u)],
+                                     e2 = E[BE::at(2, az, bz, w)];
+                            const RT y12 = yv * e1 * e2, y02 = yv * e0 * e2, y01 = yv * e0 * e1;
+                            dA[0] += y12 * Db[BD::at(0, 0, ax, bx, t)];
+                            dA[1] += y02 * Db[BD::at(0, 1, ay, by, u)];
+                            dA[2] += y01 * Db[BD::at(0, 2, az, bz, w)];
+                            dB[0] += y12 * Db[BD::at(1, 0, ax, bx, t)];
+                            dB[1] += y02 * Db[BD::at(1, 1, ay, by, u)];
+                            dB[2] += y01 * Db[BD::at(1, 2, az, bz, w)];
+                        }
+            }
+        }
+    }
+}
+
+// Register footprint of the hoisted order (Gamma column, Y and the summed
+// ket step per contraction group), in bytes: used where it fits.
 template <int CX, int CY, typename RT>
+constexpr bool grad_hoist() {
+    using Q = QClass<CX, CY>;
+    return sizeof(RT) * (Q::NROW * Q::KG + Q::KG * (Q::NHB + nherm(Q::LAB + 1))) <= 800;
+}
+
+// Gradient contribution of one column; adds A, B parts to gab and C, D
+// parts to the shared accumulator gsh[natm][3]. RS: pref * R_tuv (to L + 1)
+// of the ket pair's primitive quartets staged in Rs ([ik][ib][NH(L + 1)]).
+template <int CX, int CY, typename RT, bool RS = false>
 __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStageT<RT>& st, int P2, double QQ, int ic,
-                                            int id, int kg, double (&gab)[6], double* gsh) {
+                                            int id, int kg, double (&gab)[6], double* gsh,
+                                            const RT* __restrict__ Rs = nullptr) {
     using Q = QClass<CX, CY>;
     using BE = BraE<Q::LA, Q::LB, 1>;
     using BD = BraD<Q::LA, Q::LB>;
@@ -105,14 +319,15 @@ __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStageT<R
     double gmax = 0.0;
 #pragma unroll
     for (int kk = 0; kk < Q::KG; ++kk) {
-        const int kq = kg * Q::KG + kk, kc = kq / Q::KD, kd = kq % Q::KD;
-        const bool cv = kc < nC && kd < nD;
+        const int kq = kg * Q::KG + kk;
+        const bool cv = kq < nC * nD;
+        const int kc = cv ? kq / nD : 0, kd = cv ? kq % nD : 0;
         const size_t l = oC + kc * Q::NC + ic, sg = oD + kd * Q::ND + id;
 #pragma unroll
         for (int r = 0; r < Q::NROW; ++r) {
-            const int kab = r / Q::NAB, ab = r % Q::NAB, ka = kab / Q::KB, kb = kab % Q::KB;
+            const int kab = r / Q::NAB, ab = r % Q::NAB, ka = kab / st.nB, kb = kab % st.nB;
             double val = 0.0;
-            if (cv && ka < st.nA && kb < st.nB) {
+            if (cv && kab < st.nA * st.nB) {
                 const size_t m = st.oA + ka * Q::NA + ab / Q::NB, nb_ = st.oB + kb * Q::NB + ab % Q::NB;
                 val = __ldg(a.Dc + m * n + nb_) * __ldg(a.Dc + l * n + sg);
                 for (int x = 0; x < a.nx; ++x) {
@@ -134,6 +349,10 @@ __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStageT<R
 #pragma unroll
         for (int kk = 0; kk < Q::KG; ++kk) Gr[r][kk] = static_cast<RT>(G[r][kk]);
     RT dA[3] = {0.0, 0.0, 0.0}, dB[3] = {0.0, 0.0, 0.0}, dC[3] = {0.0, 0.0, 0.0};
+    if constexpr (grad_hoist<CX, CY, RT>()) {
+        grad_prims_hoisted<CX, CY, RT, RS>(st, Gr, a.q.pv.rec + a.q.pv.slot[P2] * PPW, a.q.pv.npp[P2], ic, id, kg,
+                                           dA, dB, dC, Rs);
+    } else {
     const int cx = cart_x(LC, ic), cy = cart_y(LC, ic), cz = cart_z(LC, ic);
     const int dx = cart_x(LD, id), dy = cart_y(LD, id), dz = cart_z(LD, id);
     const RT fcd = cart_norm(cx, cy, cz) * cart_norm(dx, dy, dz);
@@ -164,14 +383,10 @@ __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStageT<R
         }
         for (int ib = 0; ib < st.nbp; ++ib) {
             const RT* sb = st.SB + ib * SBW;
-            const RT p = sb[0];
-            const RT rs = rsqrt_t(p + q);
-            const RT alpha = p * q * rs * rs;
-            const RT pref = RT(TWO_PI_2_5) * sb[1] * iq * rs;
             const RT* E = st.E + (size_t)ib * BE::SIZE;
             const RT* Db = st.D + (size_t)ib * BD::SIZE;
-            RT R[nherm(L)];
-            hermite_r<L>(alpha, sb[2] - k.Qx, sb[3] - k.Qy, sb[4] - k.Qz, R);
+            // everything below is linear in pref * R_tuv (R up to L + 1)
+            auto body = [&](const auto& R, RT pref) {
             // Gamma contracted with this bra primitive's coefficients and f_ab,
             // then summed over the ket contractions: gq[ab] = sum_kk gb[ab][kk] ck[kk]
             RT gq[Q::NAB];
@@ -281,7 +496,20 @@ __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStageT<R
                         dC[1] += yv * s1;
                         dC[2] += yv * s2;
                     }
+            };
+            if constexpr (RS) {
+                body(Rs + (size_t)(ik * st.nbp + ib) * nherm(L), RT(1));
+            } else {
+                const RT p = sb[0];
+                const RT rs = rsqrt_t(p + q);
+                const RT alpha = p * q * rs * rs;
+                const RT pref = RT(TWO_PI_2_5) * sb[1] * iq * rs;
+                RT R[nherm(L)];
+                hermite_r<L>(alpha, sb[2] - k.Qx, sb[3] - k.Qy, sb[4] - k.Qz, R);
+                body(R, pref);
+            }
         }
+    }
     }
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
@@ -297,10 +525,19 @@ __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStageT<R
 // block quartet, deg [|Dc|_AB |Dc|_CD + |k|/2 nx (|Dx|_AC |Dx|_BD +
 // |Dx|_AD |Dx|_BC)] >= max|Gamma|, can reach the threshold and the quartet
 // is not one-centre; the exact per-column test follows in grad_column.
+#ifndef AIMD_GRAD_RSMEM_MINL
+#define AIMD_GRAD_RSMEM_MINL 4
+#endif
+// Two-stage items (R_tuv to L + 1 staged per primitive quartet) for the
+// gradient of class pair (CX, CY).
+template <int CX, int CY>
+constexpr bool grad_rsmem() { return CY >= 1 && QClass<CX, CY>::L + 1 >= AIMD_GRAD_RSMEM_MINL; }
+
 template <int CX, int CY, typename RT>
 __device__ __forceinline__ void grad_ket_class(const GradArgs& a, const BraStageT<RT>& st, int spos, double (&gab)[6],
-                                               double* gsh, KetQueue& kq, int& rot) {
+                                               double* gsh, KetQueueR& kq, int& rot, RT* Rbuf) {
     using Q = QClass<CX, CY>;
+    constexpr bool RS = grad_rsmem<CX, CY>();
     const double q1 = a.q.sortedQ[spos];
     const int nb = a.nblock;
     const double xf = 0.5 * fabs(a.kfac) * a.nx;
@@ -320,12 +557,19 @@ __device__ __forceinline__ void grad_ket_class(const GradArgs& a, const BraStage
             const double deg = 0.5 * (st.A != st.B ? 2.0 : 1.0) * (C != Dd ? 2.0 : 1.0) * (st.P1 != P2 ? 2.0 : 1.0);
             return q1 * a.q.sortedQ[pos] * deg * gb >= a.thr;
         };
-        auto work = [&](int pos, int r) {
-            const int kg = r % Q::NKG, cd = r / Q::NKG;
-            grad_column<CX, CY, RT>(a, st, a.q.sorted[pos], q1 * a.q.sortedQ[pos], cd / Q::ND, cd % Q::ND, kg, gab,
-                                    gsh);
+        const int nkg = seg_groups<Q::KG, Q::NKG>(sub);
+        auto work = [&](int pos, int r, const RT* Rs) {
+            const int kg = r % nkg, cd = r / nkg;
+            grad_column<CX, CY, RT, RS>(a, st, a.q.sorted[pos], q1 * a.q.sortedQ[pos], cd / Q::ND, cd % Q::ND, kg,
+                                        gab, gsh, Rs);
         };
-        ket_items<Q::NCD * Q::NKG>(a.q.seg_start[seg] + static_cast<int>(kb), ke - kb, kq, rot, keep, work);
+        const int j0 = a.q.seg_start[seg] + static_cast<int>(kb);
+        if constexpr (RS) {
+            ket_items_r<Q::L + 1>(Q::NCD * nkg, j0, ke - kb, kq, rot, st, a.q, Rbuf, keep, work);
+        } else {
+            ket_items(Q::NCD * nkg, j0, ke - kb, kq, rot, keep,
+                      [&](int pos, int r) { work(pos, r, static_cast<const RT*>(nullptr)); });
+        }
     }
 }
 
@@ -342,9 +586,10 @@ __global__ void __launch_bounds__(128, AIMD_GRAD_MINB) grad2e_bra_kernel(GradArg
     using Q0 = QClass<CX, 0>;
     extern __shared__ double smem[];
     double* gsh = smem;
-    RT* Esm = reinterpret_cast<RT*>(smem + 3 * a.natm);
+    RT* Rbuf = reinterpret_cast<RT*>(smem + 3 * a.natm);
+    RT* Esm = Rbuf + a.rbuf;
     __shared__ BraStageT<RT> st;
-    __shared__ KetQueue kq;
+    __shared__ KetQueueR kq;
     __shared__ int any;
     const int spos = a.q.cls_start[CX] + blockIdx.x;
     if (threadIdx.x == 0) {
@@ -367,7 +612,7 @@ __global__ void __launch_bounds__(128, AIMD_GRAD_MINB) grad2e_bra_kernel(GradArg
     __syncthreads();
     double gab[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     int rot = 0;
-    grad_ket_class<CX, CY, RT>(a, st, spos, gab, gsh, kq, rot);
+    grad_ket_class<CX, CY, RT>(a, st, spos, gab, gsh, kq, rot, Rbuf);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         if (gab[d] != 0.0) atomicAdd(gsh + 3 * st.aA + d, gab[d]);
@@ -378,11 +623,20 @@ __global__ void __launch_bounds__(128, AIMD_GRAD_MINB) grad2e_bra_kernel(GradArg
         if (gsh[i] != 0.0) atomicAdd(a.grad + i, gsh[i]);
 }
 
+// Elements of the staged-R buffer of the (CX, CY) gradient kernel.
+template <int CX, int CY, typename RT>
+size_t grad_rbuf_elems(int max_bra_prims, int max_ket_prims) {
+    if constexpr (grad_rsmem<CX, CY>())
+        return rsmem_bytes<QClass<CX, CY>::L + 1, RT>(max_bra_prims, max_ket_prims) / sizeof(RT);
+    return 0;
+}
+
 template <int CX, typename RT>
-size_t grad_smem_bytes(int natm, int max_bra_prims) {
+size_t grad_smem_bytes(int natm, int max_bra_prims, size_t rbuf_elems) {
     using Q0 = QClass<CX, 0>;
     return sizeof(double) * 3 * (size_t)natm +
-           sizeof(RT) * (size_t)max_bra_prims * (BraE<Q0::LA, Q0::LB, 1>::SIZE + BraD<Q0::LA, Q0::LB>::SIZE + SBW);
+           sizeof(RT) * (rbuf_elems + (size_t)max_bra_prims * (BraE<Q0::LA, Q0::LB, 1>::SIZE +
+                                                              BraD<Q0::LA, Q0::LB>::SIZE + SBW));
 }
 
 }  // namespace hf

@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -84,6 +85,9 @@ struct aimd_ctx {
     void* cub_tmp;
     size_t cub_bytes;
     double* pos;            // [natm][3] device copy of the current geometry
+    // J/K: bra K rows in global memory for every class (otherwise only where
+    // the shared rows would not fit); AIMD_JK_GLOBAL_K_ROWS=1 at creation
+    int jk_global_rows = 0;
     bool have_geometry = false;
     uint64_t launches = 0;
 };
@@ -111,6 +115,10 @@ extern "C" int aimd_create(aimd_ctx** out, int natm, int nao, int nblock, const 
             return AIMD_ERR_UNSUPPORTED;
         }
     auto* c = new aimd_ctx();
+    {
+        const char* kg = getenv("AIMD_JK_GLOBAL_K_ROWS");
+        c->jk_global_rows = kg && kg[0] == '1' ? 1 : 0;
+    }
     c->natm = natm;
     c->nao = nao;
     c->nblock = nblock;
@@ -263,7 +271,7 @@ namespace {
 // Primitive pairs of each block pair with mu |A-B|^2 <= 50 (the reference's
 // PRIM_CUTOFF, aimd/qc/integrals.py:506-510), compacted into the pair's slot.
 __global__ void pair_prep_kernel(int npair, const int* pa, const int* pb, const int64_t* slot, const int* blk_atom,
-                                 const int* blk_l, const int* blk_p0, const int* blk_np, const double* exps,
+                                 const int* blk_ncon, const int* blk_p0, const int* blk_np, const double* exps,
                                  const double* coefs, const double* pos, int* npp, double* rec) {
     const int ip = blockIdx.x * blockDim.x + threadIdx.x;
     if (ip >= npair) return;
@@ -272,7 +280,9 @@ __global__ void pair_prep_kernel(int npair, const int* pa, const int* pb, const 
     const double ABx = pos[3 * iA] - pos[3 * iB], ABy = pos[3 * iA + 1] - pos[3 * iB + 1],
                  ABz = pos[3 * iA + 2] - pos[3 * iB + 2];
     const double r2 = ABx * ABx + ABy * ABy + ABz * ABz;
-    const int kB = ncon_cap(blk_l[B]);
+    // contraction products in compact order: index ca * nB + cb over the
+    // block's actual contractions (ca < nA, cb < nB), zeros after them
+    const int nA = blk_ncon[A], nB = blk_ncon[B];
     double* out = rec + slot[ip] * PPW;
     int n = 0;
     for (int ka = blk_p0[A]; ka < blk_p0[A] + blk_np[A]; ++ka) {
@@ -295,8 +305,8 @@ __global__ void pair_prep_kernel(int npair, const int* pa, const int* pb, const 
             r[10] = ap * ABy;
             r[11] = ap * ABz;
             for (int i = 0; i < 4; ++i) r[12 + i] = 0.0;
-            for (int ca = 0; ca < ncon_cap(blk_l[A]); ++ca)
-                for (int cb = 0; cb < kB; ++cb) r[12 + ca * kB + cb] = coefs[2 * ka + ca] * coefs[2 * kb + cb];
+            for (int ca = 0; ca < nA; ++ca)
+                for (int cb = 0; cb < nB; ++cb) r[12 + ca * nB + cb] = coefs[2 * ka + ca] * coefs[2 * kb + cb];
             ++n;
         }
     }
@@ -493,8 +503,8 @@ int class_status(aimd_ctx* c, cudaError_t r, const char* what, int cl, int nlaun
         return AIMD_OK;
     }
     if (r == cudaErrorInvalidConfiguration) {
-        snprintf(g_err, sizeof g_err, "%s (pair class %d): shared memory beyond the 227 KB per-CTA limit "
-                 "(too many AOs for the K-row accumulator)", what, cl);
+        snprintf(g_err, sizeof g_err, "%s (pair class %d): shared memory beyond the 227 KB per-CTA limit",
+                 what, cl);
         return AIMD_ERR_UNSUPPORTED;
     }
     snprintf(g_err, sizeof g_err, "%s (pair class %d): %s", what, cl, cudaGetErrorString(r));
@@ -566,7 +576,7 @@ extern "C" int aimd_set_geometry(aimd_ctx* c, const double* pos, void* stream) {
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     CK(cudaMemcpyAsync(c->pos, pos, 3 * sizeof(double) * c->natm, cudaMemcpyDefault, st));
     const int np = c->npair;
-    pair_prep_kernel<<<(np + 127) / 128, 128, 0, st>>>(np, c->pa, c->pb, c->slot, c->blk_atom, c->blk_l, c->blk_p0,
+    pair_prep_kernel<<<(np + 127) / 128, 128, 0, st>>>(np, c->pa, c->pb, c->slot, c->blk_atom, c->blk_ncon, c->blk_p0,
                                                         c->blk_np, c->blk_exp, c->blk_coef, c->pos, c->npp, c->rec);
     ++c->launches;
     CK(cudaGetLastError());
@@ -629,6 +639,8 @@ extern "C" int aimd_jk(aimd_ctx* c, int nset, const double* D, double* J, double
         a.bmax = nullptr;
         a.nblock = c->nblock;
         a.dthr = 0.0;
+        a.rbuf = 0;
+        a.kglobal = c->jk_global_rows;
 #define AIMD_JK(X, S) first_error(launch_jk_c##X(e, a, S), mixed ? launch_jk32_c##X(e, a, S) : cudaSuccess)
 #define AIMD_NL(X) jk_launches(c, X, mixed)
         AIMD_EACH_CLASS_CONCURRENT(AIMD_JK, "aimd_jk", AIMD_NL);
@@ -696,6 +708,8 @@ extern "C" int aimd_jk_delta(aimd_ctx* c, int nset, const double* D, double* J, 
         a.bmax = c->bmax;
         a.nblock = c->nblock;
         a.dthr = dthr;
+        a.rbuf = 0;
+        a.kglobal = c->jk_global_rows;
 #define AIMD_JK(X, S) first_error(launch_jk_c##X(e, a, S), mixed ? launch_jk32_c##X(e, a, S) : cudaSuccess)
 #define AIMD_NL(X) jk_launches(c, X, mixed)
         AIMD_EACH_CLASS_CONCURRENT(AIMD_JK, "aimd_jk_delta", AIMD_NL);
@@ -705,11 +719,23 @@ extern "C" int aimd_jk_delta(aimd_ctx* c, int nset, const double* D, double* J, 
     return AIMD_OK;
 }
 
+namespace {
+// The tensor probes evaluate every quartet in FP64 whatever FP32 cutoff the
+// context carries: the cutoff is set aside for the probe and put back after.
+struct Fp64Probe {
+    aimd_ctx* c;
+    double saved;
+    explicit Fp64Probe(aimd_ctx* ctx) : c(ctx), saved(ctx->fp32_cutoff) { c->fp32_cutoff = 0.0; }
+    ~Fp64Probe() { c->fp32_cutoff = saved; }
+};
+}  // namespace
+
 // Test and debug sizes only: the tensor is probed column by column through
 // the integral-direct Coulomb build (J[D] with D the symmetric unit matrix
 // of (l, s) gives (mn|ls)); scratch for D/J/K is allocated here.
 extern "C" int aimd_eri_tensor(aimd_ctx* c, double* eri, double thr, void* stream) {
     if (!c || !eri || !c->have_geometry) return AIMD_ERR_ARG;
+    const Fp64Probe fp64(c);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int n = c->nao;
     const size_t nn = (size_t)n * n;
@@ -794,6 +820,7 @@ extern "C" int aimd_eri_tensor_static(aimd_ctx* c, double* eri, double thr, void
     }
     double* scratch = nullptr;
     if (int r = eri_static_scratch(&scratch)) return r;
+    const Fp64Probe fp64(c);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const size_t nn = (size_t)n * n;
     double *D = scratch, *J = scratch + nn, *K = scratch + 2 * nn;
@@ -844,6 +871,7 @@ extern "C" int aimd_grad2e(aimd_ctx* c, const double* Dc, int nx, const double* 
     a.thr = thr;
     a.grad = grad;
     a.natm = c->natm;
+    a.rbuf = 0;
     a.bmc = c->bmc;
     a.bmx = c->bmx;
     a.nblock = c->nblock;

@@ -50,10 +50,25 @@ cudaError_t launch_onee(const LaunchEnv& e, const ShellView& sv, const int* sp_c
 cudaError_t launch_onee_grad(const LaunchEnv& e, const ShellView& sv, const int* sp_cls_start, const double* W,
                              const double* D, double* grad, cudaStream_t st, int* nlaunch);
 
+constexpr size_t kSmemLimit = 227 * 1024;     // dynamic shared memory per CTA (sm_100a)
+
+// Allow `bytes` of dynamic shared memory for `kernel`. The default limit is
+// 48 KB for static plus dynamic shared memory together, so the opt-in is
+// needed whenever the sum passes it; the sum may not pass kSmemLimit.
 inline cudaError_t set_smem_limit(const void* kernel, size_t bytes) {
-    if (bytes > 227 * 1024) return cudaErrorInvalidConfiguration;
-    if (bytes > 48 * 1024) return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+    if (e != cudaSuccess) return e;
+    if (bytes + fa.sharedSizeBytes > kSmemLimit) return cudaErrorInvalidConfiguration;
+    if (bytes + fa.sharedSizeBytes > 48 * 1024)
+        return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     return cudaSuccess;
+}
+
+// Static shared memory of `kernel` (0 if the query fails).
+inline size_t static_smem(const void* kernel) {
+    cudaFuncAttributes fa;
+    return cudaFuncGetAttributes(&fa, kernel) == cudaSuccess ? fa.sharedSizeBytes : 0;
 }
 
 }  // namespace hf

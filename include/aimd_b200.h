@@ -66,6 +66,10 @@ int aimd_set_fp32_cutoff(aimd_ctx *ctx, double cutoff);
 /* Integral-direct J/K for nset symmetric densities D[nset][nao][nao]
  * (device). Writes the un-symmetrised accumulators: the caller forms
  * J = J + J^T and K = K + K^T. Quartets with Q1 Q2 < thr are skipped.
+ * The K rows of a bra pair's functions are accumulated per CTA in shared
+ * memory, or in global memory where they would not fit (large bases; every
+ * class when the environment variable AIMD_JK_GLOBAL_K_ROWS=1 is set at
+ * aimd_create, a test switch). No size limit on nao from this.
  * Replaces eri_tensor + jk_from_eri (aimd/qc/integrals.py:986-1044). */
 int aimd_jk(aimd_ctx *ctx, int nset, const double *D, double *J, double *K, double thr, void *stream);
 
@@ -78,7 +82,9 @@ int aimd_jk(aimd_ctx *ctx, int nset, const double *D, double *J, double *K, doub
 int aimd_jk_delta(aimd_ctx *ctx, int nset, const double *D, double *J, double *K, double thr, double dthr,
                   void *stream);
 
-/* Full screened tensor eri[nao^4] (device), test/debug sizes only.
+/* Full screened tensor eri[nao^4] (device), test/debug sizes only. Every
+ * quartet is evaluated in FP64 whatever aimd_set_fp32_cutoff set; the
+ * context's cutoff is unchanged afterwards.
  * aimd/qc/integrals.py:986-1006 (eri_tensor). */
 int aimd_eri_tensor(aimd_ctx *ctx, double *eri, double thr, void *stream);
 
@@ -88,9 +94,12 @@ int aimd_eri_tensor(aimd_ctx *ctx, double *eri, double thr, void *stream);
  * No counterpart in the reference.
  *   - nao <= AIMD_ERI_STATIC_MAX_NAO (128, 384 KiB of scratch per device);
  *     larger sizes return AIMD_ERR_ARG with a message, before any work;
+ *   - every quartet in FP64, as aimd_eri_tensor;
  *   - the context's device must be current; the first call on each device
  *     looks up the scratch address (cudaGetSymbolAddress) and should come
- *     before any stream capture;
+ *     before any stream capture; the address is kept for the life of the
+ *     process, so the library must not be used across a cudaDeviceReset of
+ *     that device;
  *   - nothing has to be zeroed by the caller; asynchronous on stream (the
  *     tensor is ready when the stream is), unlike aimd_eri_tensor;
  *   - the scratch is one per device: calls that overlap on one device (other

@@ -154,11 +154,14 @@ def eri_tensor(basis: BasisSet, schwarz_threshold: float = DEFAULT_SCHWARZ) -> n
     return eri
 
 
-def jk_direct(basis: BasisSet, densities: np.ndarray, schwarz_threshold: float = DEFAULT_SCHWARZ):
+def jk_direct(basis: BasisSet, densities: np.ndarray, schwarz_threshold: float = DEFAULT_SCHWARZ,
+              stride: int = 1, offset: int = 0):
     """
     J, K of aimd/qc/integrals.py:1031-1044 (jk_from_eri of the screened
     tensor) without storing the tensor. Densities may be non-symmetric:
     J depends on the symmetric part only, K = A(D) + A(D^T)^T.
+    stride > 1 evaluates only the quartets of bra pairs p1 = offset (mod
+    stride): a timing sample, not J/K.
     """
     D = np.asarray(densities, dtype=float)
     single = D.ndim == 2
@@ -170,8 +173,9 @@ def jk_direct(basis: BasisSet, densities: np.ndarray, schwarz_threshold: float =
     n = basis.nao
     Ja = np.zeros_like(Din)
     Ka = np.zeros_like(Din)
-    lib().orc_jk_direct(*pr.args(), _p(Q), ctypes.c_double(schwarz_threshold), ctypes.c_int64(n),
-                        ctypes.c_int64(Din.shape[0]), _p(Din), _p(Ja), _p(Ka))
+    lib().orc_jk_direct_strided(*pr.args(), _p(Q), ctypes.c_double(schwarz_threshold), ctypes.c_int64(n),
+                                ctypes.c_int64(Din.shape[0]), _p(Din), _p(Ja), _p(Ka), ctypes.c_int64(stride),
+                                ctypes.c_int64(offset))
     if sym:
         J = Ja + Ja.transpose(0, 2, 1)
         K = Ka + Ka.transpose(0, 2, 1)
@@ -191,17 +195,18 @@ def _sym(D, nao, what):
 
 
 def two_electron_gradient(basis: BasisSet, D_coulomb, D_exchange_list, k_factor,
-                          schwarz_threshold: float = DEFAULT_SCHWARZ_GRAD) -> np.ndarray:
-    """aimd/qc/integrals.py:1498-1520"""
+                          schwarz_threshold: float = DEFAULT_SCHWARZ_GRAD, stride: int = 1,
+                          offset: int = 0) -> np.ndarray:
+    """aimd/qc/integrals.py:1498-1520 (stride > 1: bra pairs offset mod stride only, a timing sample)"""
     n = basis.nao
     Dc = _sym(D_coulomb, n, "D_coulomb")
     Dx = np.ascontiguousarray(np.array([_sym(d, n, "D_exchange") for d in D_exchange_list]).reshape(-1, n, n))
     pr = pairs(basis)
     Q = schwarz_bounds(basis)
     g = np.zeros((basis.natm, 3))
-    lib().orc_grad2e(*pr.args(), _p(Q), ctypes.c_double(schwarz_threshold), ctypes.c_int64(n),
-                     ctypes.c_int64(basis.natm), _p(Dc), ctypes.c_int64(Dx.shape[0]), _p(Dx),
-                     ctypes.c_double(k_factor), _p(g))
+    lib().orc_grad2e_strided(*pr.args(), _p(Q), ctypes.c_double(schwarz_threshold), ctypes.c_int64(n),
+                             ctypes.c_int64(basis.natm), _p(Dc), ctypes.c_int64(Dx.shape[0]), _p(Dx),
+                             ctypes.c_double(k_factor), _p(g), ctypes.c_int64(stride), ctypes.c_int64(offset))
     return g
 
 
@@ -585,7 +590,8 @@ def flop_model(basis: BasisSet, threshold: float = DEFAULT_SCHWARZ) -> dict:
     def NH(L):
         return (L + 1) * (L + 2) * (L + 3) // 6
 
-    total = 0.0
+    rtab = np.array([sum(NH(L0 - n) for n in range(L0 + 1)) for L0 in range(2 * int(l.max(initial=0)) * 2 + 1)])
+    per_bra = np.zeros(pr.npair)
     nq = 0.0
     for p1 in range(pr.npair):
         p2 = np.arange(p1 + 1)
@@ -594,10 +600,11 @@ def flop_model(basis: BasisSet, threshold: float = DEFAULT_SCHWARZ) -> dict:
         if p2.size == 0:
             continue
         Lb, Lk = Lp[p1], Lp[p2]
-        L = Lb + Lk
-        rsum = np.array([sum(NH(L0 - n) for n in range(L0 + 1)) for L0 in range(9)])[L]
+        rsum = rtab[Lb + Lk]
         per = 2 * rsum + 2 * NH(Lb) * NH(Lk) * nab[p2] * ncon[p2] + 2 * NH(Lb) * nab[p1] * nab[p2] * ncon[p2]
         w = npp[p1] * npp[p2]
-        total += float(np.sum(per * w))
+        per_bra[p1] = float(np.sum(per * w))
         nq += float(np.sum(w))
-    return {"flop": total, "prim_quartets": nq}
+    # per_bra[p1]: the flops of bra pair p1's quartets (the unit the strided
+    # samples of jk_direct / two_electron_gradient select)
+    return {"flop": float(per_bra.sum()), "prim_quartets": nq, "per_bra": per_bra}

@@ -540,8 +540,18 @@ void orc_eri_tensor(PAIR_ARGS, const double *Q, double threshold, i64 nao, doubl
  * with g = 1 / n_gen, n_gen = the number of times the block visits each
  * tensor element under the 8 index maps; J = Jacc + Jacc^T and, for symmetric D, K = Kacc + Kacc^T
  * (reference result jk_from_eri(eri_tensor, D), integrals.py:1009-1044). */
+/* Bra pairs p1 with p1 % stride == offset only (stride 1: the whole build);
+ * the bench times strided samples of one build on the host cores. */
+void orc_jk_direct_strided(PAIR_ARGS, const double *Q, double threshold, i64 nao, i64 nset, const double *D,
+                           double *Jacc, double *Kacc, i64 stride, i64 offset);
+
 void orc_jk_direct(PAIR_ARGS, const double *Q, double threshold, i64 nao, i64 nset, const double *D,
                    double *Jacc, double *Kacc) {
+    orc_jk_direct_strided(PAIR_PASS, Q, threshold, nao, nset, D, Jacc, Kacc, 1, 0);
+}
+
+void orc_jk_direct_strided(PAIR_ARGS, const double *Q, double threshold, i64 nao, i64 nset, const double *D,
+                           double *Jacc, double *Kacc, i64 stride, i64 offset) {
     init_tables();
     Pairs pr = make_pairs(PAIR_PASS);
     i64 n2 = nao * nao, tot = nset * n2;
@@ -559,7 +569,7 @@ void orc_jk_direct(PAIR_ARGS, const double *Q, double threshold, i64 nao, i64 ns
         double *J = acc + (size_t)tid * 2 * tot, *K = J + tot;
         Scratch s = scratch_new(&pr, 0);
 #pragma omp for schedule(dynamic, 1)
-        for (i64 p1 = 0; p1 < pr.npair; p1++)
+        for (i64 p1 = offset; p1 < pr.npair; p1 += stride)
             for (i64 p2 = 0; p2 <= p1; p2++) {
                 if (Q[p1] * Q[p2] < threshold) continue;
                 int sw = quartet_swapped(&pr, p1, p2);
@@ -664,8 +674,17 @@ static void grad_pass(const Pairs *pr, i64 pb, i64 pk, const double *G, i64 gs, 
 }
 
 /* integrals.py:1247-1369 (_eri_grad_kernel) + :1498-1520 (two_electron_gradient) */
+void orc_grad2e_strided(PAIR_ARGS, const double *Q, double threshold, i64 nao, i64 natm, const double *Dc, i64 nx,
+                        const double *Dx, double kfac, double *grad, i64 stride, i64 offset);
+
 void orc_grad2e(PAIR_ARGS, const double *Q, double threshold, i64 nao, i64 natm, const double *Dc, i64 nx,
                 const double *Dx, double kfac, double *grad) {
+    orc_grad2e_strided(PAIR_PASS, Q, threshold, nao, natm, Dc, nx, Dx, kfac, grad, 1, 0);
+}
+
+/* bra pairs pb with pb % stride == offset only (stride 1: the whole gradient) */
+void orc_grad2e_strided(PAIR_ARGS, const double *Q, double threshold, i64 nao, i64 natm, const double *Dc, i64 nx,
+                        const double *Dx, double kfac, double *grad, i64 stride, i64 offset) {
     init_tables();
     Pairs pr = make_pairs(PAIR_PASS);
     int nthr = 1;
@@ -685,7 +704,7 @@ void orc_grad2e(PAIR_ARGS, const double *Q, double threshold, i64 nao, i64 natm,
         double *G = malloc(sizeof(double) * mr * mr), *Gt = malloc(sizeof(double) * mr * mr);
         double gab[6], gcd[6];
 #pragma omp for schedule(dynamic, 1)
-        for (i64 pb = 0; pb < pr.npair; pb++) {
+        for (i64 pb = offset; pb < pr.npair; pb += stride) {
             i64 si = pr.pair_blocks[2 * pb], sj = pr.pair_blocks[2 * pb + 1];
             i64 aA = pr.blk_atom[si], aB = pr.blk_atom[sj];
             for (i64 pk = 0; pk <= pb; pk++) {

@@ -4,10 +4,13 @@ implementation (Nathan-W123/Ab-Initio-MD, numba CPU code) on the benchmark
 geometries. The reference is importable only where its source tree is
 available, so the fixtures are committed and the tests read them.
 
-    NUMBA_CACHE_DIR=/tmp/numba_cache python tests/golden/make_golden.py /path/to/reference [--only=case1,case2]
+    NUMBA_CACHE_DIR=<writable dir> python tests/golden/make_golden.py <reference source tree> [--only=case1,case2]
 
 Fixtures (all arrays float64, Hartree atomic units):
   boys.npz            F_0..F_32 at 60 arguments (aimd/qc/boys.py:143)
+  basis_arrays.npz    the reference BasisSet's flat shell / primitive /
+                      block arrays for several molecules and basis sets
+                      (the host layout must match them bitwise)
   <case>.npz          positions, Schwarz bounds, a sample of ERIs, J/K of
                       random densities, one-electron matrices, two- and
                       one-electron gradient contractions at fixed
@@ -61,7 +64,9 @@ def main() -> None:
     args = [a for a in sys.argv[1:] if not a.startswith("--only=")]
     only = [a.split("=", 1)[1].split(",") for a in sys.argv[1:] if a.startswith("--only=")]
     only = set(only[0]) if only else None
-    ref = args[0] if args else "/root/reference"
+    if not args:
+        sys.exit("usage: make_golden.py <reference source tree> [--only=case1,case2]")
+    ref = args[0]
     sys.path.insert(0, ref)
     sys.path.insert(0, os.path.join(REPO, "ab-initio-md_b200"))
     from aimd.qc import integrals as I
@@ -77,6 +82,8 @@ def main() -> None:
     if only is None:
         F = np.array([boys(32, float(x)) for x in xs])
         np.savez_compressed(os.path.join(HERE, "boys.npz"), x=xs, F=F)
+    if only is None or "basis_arrays" in only:
+        _basis_arrays(build_basis, G)
 
     cases = {
         "water_631gs": (*G.water(), "6-31g*", 0, 1, {}),
@@ -144,6 +151,32 @@ def main() -> None:
             out["W"] = energy_weighted_density(res.spin_densities, res.fock)
         print(f"  nao {n} E {res.energy:.12f} it {res.iterations} flop {flop:.3e}", flush=True)
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+
+
+BASIS_ARRAYS = ("shell_atom", "shell_l", "shell_prim", "shell_ao", "prim_exp", "prim_coef", "blk_shell", "blk_atom",
+                "blk_l", "blk_ncon", "blk_ao", "blk_prim", "blk_exp", "blk_coef", "ao_lxyz", "atom_ao")
+
+
+def _basis_arrays(build_basis, G) -> None:
+    """The reference BasisSet arrays of several molecules, keyed '<case>/<array>'."""
+    mols = {
+        "water_sto3g": (*G.water(), "sto-3g"),
+        "water_631gs": (*G.water(), "6-31g*"),
+        "methanol_631gss": (*G.methanol(), "6-31g**"),
+        "water2_ccpvdz": (*G.water_cluster(2, seed=4), "cc-pvdz"),
+        "h2s_631gs": (["S", "H", "H"], _bent(1.336, 92.1), "6-31g*"),
+        "hcl_ccpvdz": (["Cl", "H"], np.array([[0.0, 0.0, 0.0], [0.0, 0.0, 1.2746 * ANG]]), "cc-pvdz"),
+        "ch3no_631g": (["C", "H", "H", "H", "N", "O"], np.arange(18, dtype=float).reshape(6, 3) * 0.7, "6-31g"),
+    }
+    out = {}
+    for name, (sym, pos, basis) in mols.items():
+        b = build_basis(sym, pos, basis)
+        out[f"{name}/symbols"] = np.array(sym)
+        out[f"{name}/positions"] = np.asarray(pos, dtype=float)
+        out[f"{name}/basis"] = np.array(basis)
+        for a in BASIS_ARRAYS:
+            out[f"{name}/{a}"] = np.asarray(getattr(b, a))
+    np.savez_compressed(os.path.join(HERE, "basis_arrays.npz"), **out)
 
 
 def _bent(r_ang: float, angle_deg: float) -> np.ndarray:

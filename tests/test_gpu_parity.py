@@ -119,3 +119,54 @@ def test_jk_is_linear_and_repeatable(golden):
     Jr, Kr = I.jk(b, D1)
     np.testing.assert_allclose(Jr, J1, atol=1e-13)
     np.testing.assert_allclose(Kr, K1, atol=1e-13)
+
+
+def test_eri_tensor_is_fp64_whatever_the_context_cutoff(golden):
+    """
+    C ABI: aimd_eri_tensor evaluates every quartet in FP64 even when the
+    context carries an FP32 cutoff (here one above every Schwarz product, so
+    a J/K call would run all quartets in FP32), and leaves the cutoff set.
+    """
+    import ctypes
+
+    from aimd_b200 import _lib
+    from aimd_b200.engine import engine_for
+    g = golden("water_631gs")
+    b = _basis(g)
+    eng = engine_for(b)
+    ref = eng.eri_tensor(1e-12)
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    _lib.check(eng.lib.aimd_set_fp32_cutoff(eng.handle, ctypes.c_double(1e30)), "aimd_set_fp32_cutoff")
+    try:
+        out = torch.full_like(ref, float("nan"))
+        _lib.check(eng.lib.aimd_eri_tensor(eng.handle, ctypes.c_void_p(out.data_ptr()), ctypes.c_double(1e-12),
+                                           stream), "aimd_eri_tensor")
+        torch.cuda.synchronize()
+        assert float((out - ref).abs().max()) <= ERI_TOL
+        # the cutoff is still in force for J/K: all-FP32 quartets differ from FP64
+        D = torch.as_tensor(g["D_rand"], device="cuda")[None].contiguous()
+        J32 = torch.empty_like(D)
+        K32 = torch.empty_like(D)
+        _lib.check(eng.lib.aimd_jk(eng.handle, 1, ctypes.c_void_p(D.data_ptr()), ctypes.c_void_p(J32.data_ptr()),
+                                   ctypes.c_void_p(K32.data_ptr()), ctypes.c_double(1e-12), stream), "aimd_jk")
+        eng._fp32_cutoff = 1e30
+        J64, _ = eng.jk_acc(D, 1e-12, 0.0)
+        assert float((J32 - J64).abs().max()) > 0.0
+    finally:
+        eng._precision(0.0)
+
+
+@pytest.mark.parametrize("case", ["water_ccpvdz", "methanol_631gss"])
+def test_jk_with_k_rows_in_global_memory(golden, case, monkeypatch):
+    """
+    The J/K path that large bases take when a CTA's shared K rows (NF x nao
+    doubles) would not fit, forced here for every bra class with
+    AIMD_JK_GLOBAL_K_ROWS=1 (read when the context is created).
+    """
+    from aimd_b200 import integrals as I
+    monkeypatch.setenv("AIMD_JK_GLOBAL_K_ROWS", "1")
+    g = golden(case)
+    b = _basis(g)                      # a fresh basis object: a fresh native context
+    J, K = I.jk(b, g["D_rand"])
+    np.testing.assert_allclose(J, g["J_sym"], rtol=0, atol=ERI_TOL * 10)
+    np.testing.assert_allclose(K, g["K_sym"], rtol=0, atol=ERI_TOL * 10)

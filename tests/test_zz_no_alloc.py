@@ -50,3 +50,20 @@ def test_static_scratch_refuses_sizes_beyond_its_limit():
     assert status == _lib.AIMD_ERR_ARG
     msg = eng.lib.aimd_last_error().decode()
     assert "static scratch limit of 128" in msg
+
+
+def test_static_scratch_is_fp64_whatever_the_context_cutoff():
+    """A context that carries an FP32 cutoff still gets the FP64 tensor."""
+    sym, pos = G.water()
+    basis = build_basis(sym, pos, "6-31g*")
+    eng = engine_for(basis)
+    ref = eng.eri_tensor(THR)
+    _lib.check(eng.lib.aimd_set_fp32_cutoff(eng.handle, ctypes.c_double(1e30)), "aimd_set_fp32_cutoff")
+    eng._fp32_cutoff = 1e30
+    try:
+        out = torch.full_like(ref, float("nan"))
+        _lib.check(_static_call(eng, out), "aimd_eri_tensor_static")
+        torch.cuda.synchronize()
+        assert float((out - ref).abs().max()) <= TOL
+    finally:
+        eng._precision(0.0)
