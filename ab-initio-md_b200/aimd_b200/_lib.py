@@ -42,11 +42,51 @@ SIGNATURES = {
     "aimd_quartet_counts": (_i, [_vp, _i, _i64p]),
     "aimd_pair_data": (_i, [_vp, _i32p, _i32p, _i32p]),
     "aimd_launch_count": (ctypes.c_uint64, [_vp]),
+    "aimd_sizes": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
+    "aimd_nuclear_repulsion": (_i, [_vp, ctypes.POINTER(_d), _vp]),
     "aimd_last_error": (ctypes.c_char_p, []),
     "aimd_version": (_i, []),
 }
 
 _lib = None
+
+# the device SCF driver (include/aimd_scf.h), a second library over the first
+SCF_LIB_PATH = os.path.join(_HERE, "_native", "libaimd_scf.so")
+AIMD_SCF_CONVERGED, AIMD_SCF_MAX_ITER, AIMD_SCF_NONFINITE = 1, 2, 4
+
+
+class SCFOptions(ctypes.Structure):
+    """aimd_scf_options of include/aimd_scf.h."""
+    _fields_ = [("n_alpha", ctypes.c_int), ("n_beta", ctypes.c_int), ("unrestricted", ctypes.c_int),
+                ("max_iter", ctypes.c_int), ("diis_space", ctypes.c_int), ("conv_energy", ctypes.c_double),
+                ("conv_commutator", ctypes.c_double), ("schwarz_threshold", ctypes.c_double),
+                ("lindep_threshold", ctypes.c_double), ("max_coefficient", ctypes.c_double)]
+
+
+SCF_SIGNATURES = {
+    "aimd_scf_default_options": (None, [ctypes.POINTER(SCFOptions)]),
+    "aimd_scf_run": (_i, [_vp, ctypes.POINTER(SCFOptions), _vp, _vp, _vp, ctypes.POINTER(_d),
+                          ctypes.POINTER(_i), ctypes.POINTER(_i), _vp]),
+    "aimd_scf_release": (_i, [_vp]),
+    "aimd_scf_last_error": (ctypes.c_char_p, []),
+}
+_scf = None
+
+
+def load_scf() -> ctypes.CDLL:
+    """The SCF driver library (loaded once, after the integral library); raises if it is not built."""
+    global _scf
+    if _scf is None:
+        load()
+        if not os.path.exists(SCF_LIB_PATH):
+            raise ImportError(f"SCF driver not built: {SCF_LIB_PATH} (run aimd_b200/build.py)")
+        lib = ctypes.CDLL(SCF_LIB_PATH)
+        for name, (res, args) in SCF_SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _scf = lib
+    return _scf
 
 
 class NativeError(RuntimeError):

@@ -15,6 +15,7 @@ from __future__ import annotations
 import concurrent.futures as cf
 import glob
 import os
+import shutil
 import subprocess
 import time
 import sys
@@ -26,6 +27,10 @@ INCLUDE = os.path.join(os.path.dirname(PKG_ROOT), "include")
 OUT_DIR = os.path.join(HERE, "_native")
 OBJ_DIR = os.path.join(PKG_ROOT, "_build")
 LIB = os.path.join(OUT_DIR, "libaimd_b200.so")
+# the device SCF driver: a second library over the first, cuBLAS and cuSOLVER
+SCF_SRC = os.path.join(CSRC, "hf_scf.cu")
+SCF_OBJ = os.path.join(OBJ_DIR, "hf_scf.o")
+SCF_LIB = os.path.join(OUT_DIR, "libaimd_scf.so")
 
 NVCC = os.environ.get("NVCC", "nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
@@ -50,9 +55,28 @@ def _units() -> list[tuple[str, str, list[str]]]:
     return units
 
 
-def _newest_source() -> float:
-    files = glob.glob(os.path.join(CSRC, "*")) + glob.glob(os.path.join(INCLUDE, "*.h"))
-    return max(os.path.getmtime(f) for f in files)
+def _includes(path: str, seen: set[str]) -> set[str]:
+    """The file and every file it includes with #include "..." (transitively)."""
+    path = os.path.normpath(path)
+    if path in seen or not os.path.exists(path):
+        return seen
+    seen.add(path)
+    with open(path) as f:
+        for line in f:
+            line = line.strip()
+            if line.startswith("#include") and '"' in line:
+                inc = line.split('"')[1]
+                for base in (os.path.dirname(path), CSRC, INCLUDE):
+                    cand = os.path.join(base, inc)
+                    if os.path.exists(cand):
+                        _includes(cand, seen)
+                        break
+    return seen
+
+
+def _newest_dependency(src: str) -> float:
+    """Modification time of the newest file the unit compiles from (its source and its includes)."""
+    return max(os.path.getmtime(f) for f in _includes(src, set()))
 
 
 def _compile(unit, verbose: bool) -> str:
@@ -69,8 +93,8 @@ def _compile(unit, verbose: bool) -> str:
 def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -> str:
     os.makedirs(OUT_DIR, exist_ok=True)
     os.makedirs(OBJ_DIR, exist_ok=True)
-    newest = _newest_source()
-    todo = [u for u in _units() if force or not os.path.exists(u[1]) or os.path.getmtime(u[1]) < newest]
+    todo = [u for u in _units()
+            if force or not os.path.exists(u[1]) or os.path.getmtime(u[1]) < _newest_dependency(u[0])]
     logs = []
     if todo:
         # objects are stamped with the time the build started, so a source
@@ -84,12 +108,26 @@ def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -
             return log
         with cf.ThreadPoolExecutor(max_workers=jobs or min(len(todo), os.cpu_count() or 4)) as ex:
             logs = list(ex.map(one, todo))
+    relinked = False
     if todo or not os.path.exists(LIB):
         objs = [u[1] for u in _units()]
-        res = subprocess.run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", LIB],
-                             capture_output=True, text=True)
+        res = subprocess.run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs,
+                              "-Xlinker", "-soname=libaimd_b200.so", "-o", LIB], capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"link failed:\n{res.stderr[-4000:]}")
+        relinked = True
+    if os.path.exists(SCF_SRC):
+        stale = force or not os.path.exists(SCF_OBJ) or os.path.getmtime(SCF_OBJ) < _newest_dependency(SCF_SRC)
+        if stale:
+            logs.append(_compile((SCF_SRC, SCF_OBJ, []), verbose))
+        if stale or relinked or not os.path.exists(SCF_LIB):
+            cuda_lib = os.path.join(os.path.dirname(os.path.dirname(shutil.which(NVCC) or NVCC)), "lib64")
+            res = subprocess.run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", SCF_OBJ,
+                                  "-L", OUT_DIR, "-laimd_b200", "-L", cuda_lib, "-lcublas", "-lcusolver",
+                                  "-Xlinker", "-rpath=$ORIGIN", "-Xlinker", f"-rpath={cuda_lib}", "-o", SCF_LIB],
+                                 capture_output=True, text=True)
+            if res.returncode != 0:
+                raise RuntimeError(f"link of the SCF driver failed:\n{res.stderr[-4000:]}")
     if verbose:
         for log in logs:
             sys.stderr.write(log)

@@ -794,6 +794,72 @@ def run_device(solver: "SCFSolver", positions: np.ndarray, guess: torch.Tensor |
                           Ik.nuclear_repulsion, st["converged"], st["it"], solver.unrestricted, Ik.M)
 
 
+@dataclass(eq=False)
+class NativeSCFResult:
+    """Outcome of the C-ABI device SCF driver (include/aimd_scf.h)."""
+    energy: float
+    iterations: int
+    status: int                   # AIMD_SCF_* bits
+    spin: torch.Tensor            # (nspin, n, n) spin densities of the last Fock build
+    fock: torch.Tensor            # (nspin, n, n)
+
+    @property
+    def converged(self) -> bool:
+        from ._lib import AIMD_SCF_CONVERGED
+        return bool(self.status & AIMD_SCF_CONVERGED)
+
+
+def run_native(solver: "SCFSolver", positions: np.ndarray, guess: torch.Tensor | str | None = "sad",
+               max_iter: int | None = None) -> NativeSCFResult:
+    """
+    The SCF of ``solver`` at ``positions`` by the C-ABI device driver
+    (aimd_scf_run): the same DIIS loop in C++ over the same integral
+    kernels, for hosts that call the library without Python. ``guess``:
+    "sad" (the solver's atomic guess), None (core Hamiltonian, in the
+    driver), or a device density in the run_device protocol shape. Options
+    come from the solver's SCFOptions; incremental Fock builds, level
+    shifts and damping are not part of the driver.
+    """
+    import ctypes
+
+    from . import _lib
+    from .engine import engine_for
+    lib = _lib.load_scf()
+    Ik = solver.integrals(positions)
+    eng = engine_for(Ik.basis)
+    eng._precision(solver.options.fp32_cutoff)
+    nspin = 2 if solver.unrestricted else 1
+    n = Ik.nao
+    g = None
+    if isinstance(guess, str):
+        if guess != "sad":
+            raise ValueError(f"unknown guess {guess!r}")
+        g, _ = solver.initial_spin_densities(Ik, None)
+    elif guess is not None:
+        g = guess.to("cuda", torch.float64)
+        g = (0.5 * g)[None].expand(nspin, -1, -1) if g.dim() == 2 else (g if nspin == 2 else 0.5 * (g[0] + g[1])[None])
+    if g is not None:
+        g = g.contiguous()
+    opt = _lib.SCFOptions()
+    lib.aimd_scf_default_options(ctypes.byref(opt))
+    o = solver.options
+    opt.n_alpha, opt.n_beta, opt.unrestricted = solver.n_alpha, solver.n_beta, int(solver.unrestricted)
+    opt.max_iter = int(max_iter if max_iter is not None else o.max_iter)
+    opt.diis_space = int(o.diis_space) if o.diis else 0
+    opt.conv_energy, opt.conv_commutator = float(o.conv_energy), float(o.conv_commutator)
+    opt.schwarz_threshold = float(o.schwarz_threshold)
+    D = torch.empty((nspin, n, n), dtype=torch.float64, device="cuda")
+    F = torch.empty_like(D)
+    e, it, st = ctypes.c_double(), ctypes.c_int(), ctypes.c_int()
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    r = lib.aimd_scf_run(eng.handle, ctypes.byref(opt), ctypes.c_void_p(g.data_ptr()) if g is not None else None,
+                         ctypes.c_void_p(D.data_ptr()), ctypes.c_void_p(F.data_ptr()), ctypes.byref(e),
+                         ctypes.byref(it), ctypes.byref(st), stream)
+    if r != _lib.AIMD_OK:
+        raise _lib.NativeError(f"aimd_scf_run: status {r}: {lib.aimd_scf_last_error().decode(errors='replace')}")
+    return NativeSCFResult(float(e.value), int(it.value), int(st.value), D, F)
+
+
 def run_scf(symbols: Sequence[str], positions: np.ndarray, basis: str | BasisSet = "sto-3g", charge: int = 0,
             multiplicity: int = 1, reference: str | None = None, guess: Any = None,
             options: SCFOptions | None = None, **overrides: Any) -> SCFResult:

@@ -34,6 +34,10 @@ using RT = float;
 #define AIMD_JK_NAME AIMD_CAT(launch_jk32_c, AIMD_CLASS)
 #endif
 
+// Internal linkage: every class unit instantiates launch_one<YK> for its own
+// (class, type), and identical external names would let the linker keep one
+// unit's copy for all of them.
+namespace {
 template <int YK>
 cudaError_t launch_one(const LaunchEnv& e, const JKArgs& a0, cudaStream_t st) {
     JKArgs a = a0;
@@ -50,6 +54,7 @@ cudaError_t launch_one(const LaunchEnv& e, const JKArgs& a0, cudaStream_t st) {
     jk_bra_kernel<CX, 1, RT, YK><<<e.cls_count[CX], JK_THREADS, smem, st>>>(a);
     return cudaGetLastError();
 }
+}  // namespace
 
 // split bra classes: one launch per non-empty ket class (largest first), in
 // order on st; the others: one launch over all ket classes

@@ -69,6 +69,37 @@ __host__ __device__ inline double cart_norm(int lx, int ly, int lz) {
     return sqrt(dfact_odd(2 * (lx + ly + lz) - 1) / (dfact_odd(2 * lx - 1) * dfact_odd(2 * ly - 1) * dfact_odd(2 * lz - 1)));
 }
 
+// ---------------------------------------------------------------- accumulation
+
+// Order-independent sums: J, K and the nuclear gradients are accumulated as
+// 64-bit fixed-point integers (value * scale, rounded to nearest), so the
+// total is the same bits whatever order threads and CTAs add in (integer
+// addition is associative, and wraps modulo 2^64, so only each addend and
+// the final total need to fit in 63 bits). The float value is restored once
+// at the end. Gradients: scale 2^44 (resolution 5.7e-14 Eh/bohr, range
+// +-5.2e5). J and K: scale jk_fix_for(max |D|), 2^44 for densities of
+// magnitude 1, so that the builds of small difference densities keep the
+// relative resolution of a full build.
+typedef unsigned long long facc;
+constexpr double FIX_G = 17592186044416.0;        // 2^44
+__device__ __forceinline__ facc to_fixed(double v, double scale) {
+    return static_cast<facc>(__double2ll_rn(v * scale));
+}
+__device__ __forceinline__ void fadd(facc* p, double v, double scale) { atomicAdd(p, to_fixed(v, scale)); }
+__host__ __device__ __forceinline__ double from_fixed(facc u, double scale) {
+    return static_cast<double>(static_cast<long long>(u)) / scale;
+}
+// J/K scale for a density of largest element m in [2^(e-1), 2^e): 2^(45-e)
+// (2^44 at m = 1), e clamped to [-60, 30]. J and K are linear in D, so their
+// elements stay below 2^18 m (far above any molecular Coulomb or exchange
+// element per unit density) and every sum fits; m = 0 or NaN gives e = 0.
+__device__ __forceinline__ double jk_fix_for(double m) {
+    int e = 0;
+    if (m > 0.0 && m <= 1.0e300) frexp(m, &e);
+    e = e < -60 ? -60 : (e > 30 ? 30 : e);
+    return ldexp(1.0, 45 - e);
+}
+
 // ---------------------------------------------------------------- Boys
 
 // Coefficient a_k of the positive series F_N(x) = e^{-x} sum_k a_k (2x)^k,

@@ -21,9 +21,6 @@
 
 namespace hf {
 
-#ifndef AIMD_RSMEM_MINL
-#define AIMD_RSMEM_MINL 4
-#endif
 template <int CX, int CY>
 struct QClass {
     static constexpr int LA = cls_la(CX), LB = cls_lb(CX), LC = cls_la(CY), LD = cls_lb(CY);
@@ -39,9 +36,11 @@ struct QClass {
     static constexpr int NKG = KCD / KG;
     static constexpr int NHB = nherm(LAB);
     // R_tuv staged once per primitive quartet for all columns of a ket pair
-    // (two-stage items) when the ket pair has several columns and R is not
-    // trivially cheap
-    static constexpr bool RSMEM = CY >= 1 && L >= AIMD_RSMEM_MINL;
+    // (two-stage items): for dd bras against dp and dd kets, whose pairs have
+    // one to three primitive pairs, 18-36 columns and L = 7-8, so that the
+    // staged sub-chunks hold many items (measured: staging the classes with
+    // many-primitive pairs starved the sub-chunks and was slower)
+    static constexpr bool RSMEM = CX == 5 && CY >= 4;
 };
 
 // Bra-side E tables with an extra +G in i and j (G = 1 for gradients).
@@ -149,7 +148,7 @@ __device__ __forceinline__ void select_row(const RT (&e)[IM + 1][JM + 1][T + 1],
 // it is read from Rs, [ik][ib][NH(L)] pref * R_tuv staged by the CTA
 // (stage_r below) once for all the columns of the ket pair.
 template <int CX, int CY, typename RT, bool RS = false>
-__device__ __forceinline__ void eri_column(const BraStageT<RT>& st, const double* __restrict__ rk, int nkp, int ic,
+__device__ __forceinline__ void eri_column_bra_outer(const BraStageT<RT>& st, const double* __restrict__ rk, int nkp, int ic,
                                            int id, int kg, RT (&v)[QClass<CX, CY>::NROW][QClass<CX, CY>::KG],
                                            const RT* __restrict__ Rs = nullptr) {
     using Q = QClass<CX, CY>;
@@ -273,6 +272,123 @@ __device__ __forceinline__ void eri_column(const BraStageT<RT>& st, const double
     }
 }
 
+// Ket primitives outermost, bra primitives inner, R_tuv and the bra step per
+// primitive quartet: the order for bra pairs with many primitives (ss, ps,
+// pp), where repeating the ket setup per bra primitive would cost more than
+// the bra steps it saves.
+template <int CX, int CY, typename RT>
+__device__ __forceinline__ void eri_column_ket_outer(const BraStageT<RT>& st, const double* __restrict__ rk, int nkp,
+                                                     int ic, int id, int kg, RT (&v)[QClass<CX, CY>::NROW][QClass<CX, CY>::KG]) {
+    using Q = QClass<CX, CY>;
+    using BE = BraE<Q::LA, Q::LB, 0>;
+    constexpr int LA = Q::LA, LB = Q::LB, LC = Q::LC, LD = Q::LD, LAB = Q::LAB, LCD = Q::LCD, L = Q::L;
+    // classes with L >= 6 keep their outer Hermite loops rolled (compile time)
+    constexpr int UH = L >= 6 ? 1 : 16;
+    const int cx = cart_x(LC, ic), cy = cart_y(LC, ic), cz = cart_z(LC, ic);
+    const int dx = cart_x(LD, id), dy = cart_y(LD, id), dz = cart_z(LD, id);
+    const RT fcd = static_cast<RT>(cart_norm(cx, cy, cz) * cart_norm(dx, dy, dz));
+#pragma unroll
+    for (int r = 0; r < Q::NROW; ++r)
+#pragma unroll
+        for (int k = 0; k < Q::KG; ++k) v[r][k] = RT(0);
+    for (int ik = 0; ik < nkp; ++ik) {
+        const KetRecT<RT> k = load_ket<RT>(rk + (size_t)ik * PPW);
+        const RT q = k.a + k.b, oo2q = RT(0.5) / q, iq = RT(2) * oo2q;
+        // ket E coefficients of this column only (box t2 <= cx+dx, ...)
+        RT ex[LCD + 1], ey[LCD + 1], ez[LCD + 1];
+        {
+            RT e[LC + 1][LD + 1][LCD + 1];
+            hermite_e<LC, LD>(k.QAx, k.QBx, oo2q, k.K, e);
+            select_row<LC, LD, LCD>(e, cx, dx, ex);
+            hermite_e<LC, LD>(k.QAy, k.QBy, oo2q, RT(1), e);
+            select_row<LC, LD, LCD>(e, cy, dy, ey);
+            hermite_e<LC, LD>(k.QAz, k.QBz, oo2q, RT(1), e);
+            select_row<LC, LD, LCD>(e, cz, dz, ez);
+        }
+        RT ck[Q::KG];
+#pragma unroll
+        for (int i = 0; i < Q::KG; ++i) {
+            RT c = k.c[0];
+#pragma unroll
+            for (int j = 1; j < Q::KCD; ++j)
+                if (j == kg * Q::KG + i) c = k.c[j];
+            ck[i] = c * fcd;
+        }
+        for (int ib = 0; ib < st.nbp; ++ib) {
+            const RT* sb = st.SB + ib * SBW;
+            const RT p = sb[0];
+            const RT rs = rsqrt_t(p + q);
+            const RT alpha = p * q * rs * rs;
+            const RT pref = RT(TWO_PI_2_5) * sb[1] * iq * rs;
+            RT R[nherm(L)];
+            hermite_r<L>(alpha, sb[2] - k.Qx, sb[3] - k.Qy, sb[4] - k.Qz, R);
+            RT X[Q::NHB];
+#pragma unroll UH
+            for (int t = 0; t <= LAB; ++t)
+#pragma unroll UH
+                for (int u = 0; u <= LAB - t; ++u)
+#pragma unroll
+                    for (int w = 0; w <= LAB - t - u; ++w) {
+                        RT s = RT(0);
+#pragma unroll
+                        for (int t2 = 0; t2 <= LCD; ++t2) {
+                            if (t2 > cx + dx) continue;
+#pragma unroll
+                            for (int u2 = 0; u2 <= LCD; ++u2) {
+                                if (u2 > cy + dy) continue;
+                                const RT exy = ((t2 + u2) & 1) ? -ex[t2] * ey[u2] : ex[t2] * ey[u2];
+#pragma unroll
+                                for (int v2 = 0; v2 <= LCD; ++v2) {
+                                    if (v2 > cz + dz) continue;
+                                    const RT e = (v2 & 1) ? -exy * ez[v2] : exy * ez[v2];
+                                    s += e * R[hidx(t + t2, u + u2, w + v2)];
+                                }
+                            }
+                        }
+                        X[hidx(t, u, w)] = pref * s;
+                    }
+            // bra step: v[(ka,kb),ab][kk] += C[ka,kb] f_ab sum_box E^{ab}_tuv X[tuv] ck[kk]
+            const RT* E = st.E + (size_t)ib * BE::SIZE;
+#pragma unroll UH
+            for (int ia = 0; ia < Q::NA; ++ia) {
+                const int ax = cart_x(LA, ia), ay = cart_y(LA, ia), az = cart_z(LA, ia);
+#pragma unroll
+                for (int jb = 0; jb < Q::NB; ++jb) {
+                    const int bx = cart_x(LB, jb), by = cart_y(LB, jb), bz = cart_z(LB, jb);
+                    const RT fab = static_cast<RT>(cart_norm(ax, ay, az) * cart_norm(bx, by, bz));
+                    RT s = RT(0);
+#pragma unroll
+                    for (int t = 0; t <= ax + bx; ++t)
+#pragma unroll
+                        for (int u = 0; u <= ay + by; ++u) {
+                            const RT exy = E[BE::at(0, ax, bx, t)] * E[BE::at(1, ay, by, u)];
+#pragma unroll
+                            for (int w = 0; w <= az + bz; ++w) s += exy * E[BE::at(2, az, bz, w)] * X[hidx(t, u, w)];
+                        }
+                    s *= fab;
+#pragma unroll
+                    for (int kab = 0; kab < Q::KAB; ++kab) {
+                        const RT c = sb[8 + kab] * s;
+#pragma unroll
+                        for (int kk = 0; kk < Q::KG; ++kk) v[kab * Q::NAB + ia * Q::NB + jb][kk] += c * ck[kk];
+                    }
+                }
+            }
+        }
+    }
+}
+
+// (row r | cd) of a quartet column: bra-outer order (the bra step once per
+// bra primitive) for the d-shell bra classes, whose pairs have few
+// primitives, and the ket-outer order for the others.
+template <int CX, int CY, typename RT, bool RS = false>
+__device__ __forceinline__ void eri_column(const BraStageT<RT>& st, const double* __restrict__ rk, int nkp, int ic,
+                                           int id, int kg, RT (&v)[QClass<CX, CY>::NROW][QClass<CX, CY>::KG],
+                                           const RT* __restrict__ Rs = nullptr) {
+    if constexpr (RS || CX >= 3) eri_column_bra_outer<CX, CY, RT, RS>(st, rk, nkp, ic, id, kg, v, Rs);
+    else eri_column_ket_outer<CX, CY, RT>(st, rk, nkp, ic, id, kg, v);
+}
+
 // Everything the quartet kernels share.
 struct QuartetArgs {
     PairView pv;
@@ -327,8 +443,9 @@ __device__ __forceinline__ void load_stage(const QuartetArgs& a, int P1, BraStag
 struct JKArgs {
     QuartetArgs q;
     const double* D;    // [nset][nao][nao], symmetric
-    double* J;          // un-symmetrised accumulators, same shape
-    double* K;
+    facc* J;            // un-symmetrised accumulators, same shape (fixed point, scale *fix)
+    facc* K;
+    const double* fix;  // device scalar: the fixed-point scale of J and K (jk_fix_for(max |D|))
     // density-weighted screening (difference densities): skip a quartet when
     // Q1 Q2 max|D| over its six density blocks < dthr; bmax = nullptr: off
     const double* bmax; // [nblock][nblock] max |D| per block pair (all sets)
@@ -353,13 +470,14 @@ template <int CX, int CY, int NS, bool KGLOBAL, typename ST>
 __device__ __forceinline__ void jk_digest_column(const JKArgs& a, const ST& st, int P2, int C, int Dd, int ic,
                                                  int id, int kg,
                                                  const double (&v)[QClass<CX, CY>::NROW][QClass<CX, CY>::KG],
-                                                 double* Jt, double* Ksm) {
+                                                 double* Jt, facc* Ksm) {
     using Q = QClass<CX, CY>;
     const BlockView& bv = a.q.bv;
     const int nC = bv.ncon[C], nD = bv.ncon[Dd], oC = bv.ao[C], oD = bv.ao[Dd];
     const double g = 1.0 / ((st.A == st.B ? 2.0 : 1.0) * (C == Dd ? 2.0 : 1.0) * (st.P1 == P2 ? 2.0 : 1.0));
     const int n = a.q.nao;
     const size_t nn = (size_t)n * n;
+    const double fx = __ldg(a.fix);
     constexpr int NFA = Q::KA * Q::NA;      // A slots, then B slots
     constexpr int NF = NFA + Q::KB * Q::NB;
 #pragma unroll
@@ -368,8 +486,8 @@ __device__ __forceinline__ void jk_digest_column(const JKArgs& a, const ST& st, 
         // K rows of the bra functions: shared accumulator, or the global K
         // itself (KGLOBAL, for bra classes whose rows would not fit)
         const bool kgl = KGLOBAL || a.kglobal;
-        double* Ks = kgl ? nullptr : Ksm + (size_t)s * NF * n;
-        double* Kg = a.K + s * nn;
+        facc* Ks = kgl ? nullptr : Ksm + (size_t)s * NF * n;
+        facc* Kg = a.K + s * nn;
 #pragma unroll
         for (int kk = 0; kk < Q::KG; ++kk) {
                 const int kq = kg * Q::KG + kk;
@@ -393,7 +511,7 @@ __device__ __forceinline__ void jk_digest_column(const JKArgs& a, const ST& st, 
                                 Jt[(s * Q::NROW + r) * blockDim.x + threadIdx.x] += 2.0 * g * v[r][kk] * dls;
                             }
                     }
-                atomicAdd(a.J + s * nn + (size_t)l * n + sg, 2.0 * g * jcd);
+                fadd(a.J + s * nn + (size_t)l * n + sg, 2.0 * g * jcd, fx);
                 // K[m, l] and K[m, sg]: rows of A's functions
 #pragma unroll
                 for (int ka = 0; ka < Q::KA; ++ka)
@@ -411,10 +529,10 @@ __device__ __forceinline__ void jk_digest_column(const JKArgs& a, const ST& st, 
                                 s1 += v[r][kk] * __ldg(D + nb_ * n + sg);
                                 s2 += v[r][kk] * __ldg(D + nb_ * n + l);
                             }
-                        double* row = kgl ? Kg + (size_t)(st.oA + ka * Q::NA + ia) * n
+                        facc* row = kgl ? Kg + (size_t)(st.oA + ka * Q::NA + ia) * n
                                               : Ks + (size_t)(ka * Q::NA + ia) * n;
-                        atomicAdd(row + l, g * s1);
-                        atomicAdd(row + sg, g * s2);
+                        fadd(row + l, g * s1, fx);
+                        fadd(row + sg, g * s2, fx);
                     }
                 // K[n, l] and K[n, sg]: rows of B's functions
 #pragma unroll
@@ -433,10 +551,10 @@ __device__ __forceinline__ void jk_digest_column(const JKArgs& a, const ST& st, 
                                 s1 += v[r][kk] * __ldg(D + m * n + sg);
                                 s2 += v[r][kk] * __ldg(D + m * n + l);
                             }
-                        double* row = kgl ? Kg + (size_t)(st.oB + kb * Q::NB + jb) * n
+                        facc* row = kgl ? Kg + (size_t)(st.oB + kb * Q::NB + jb) * n
                                               : Ks + (size_t)(NFA + kb * Q::NB + jb) * n;
-                        atomicAdd(row + l, g * s1);
-                        atomicAdd(row + sg, g * s2);
+                        fadd(row + l, g * s1, fx);
+                        fadd(row + sg, g * s2, fx);
                     }
             }
     }
@@ -445,7 +563,7 @@ __device__ __forceinline__ void jk_digest_column(const JKArgs& a, const ST& st, 
 // Items of ket class CY for the staged bra pair.
 // Work queue of one CTA: the ket pairs of a segment that pass a per-pair
 // test are compacted into shared memory in chunks of KQ_CAP (warp ballots,
-// one shared atomic per warp), then dealt to the threads as NPER items each,
+// warps in index order), then dealt to the threads as NPER items each,
 // so that lanes only receive live work. Dealing starts where the previous
 // chunk ended (rot), so ragged tails do not pile up on the low threads.
 // Every thread of the CTA must call this with the same j0 and cnt.
@@ -463,27 +581,43 @@ __device__ __forceinline__ int seg_groups(int sub) {
 }
 struct KetQueue {
     int pos[KQ_CAP];
+    int wcnt[32];           // per-warp counts of one compaction step
     int n;
 };
 
+// Compact the positions p0 .. p0+m-1 that pass keep() into q.pos[0 .. q.n)
+// in position order (per-warp ballots, warps in index order), so that the
+// queue, the item dealing and every per-thread partial sum are the same on
+// every run. store(slot, pos) records what the caller needs per entry.
+template <typename Queue, typename Keep, typename Store>
+__device__ __forceinline__ void compact(Queue& q, int p0, int m, Keep keep, Store store) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    int n = 0;
+    for (int i0 = 0; i0 < m; i0 += blockDim.x) {
+        const int i = i0 + threadIdx.x;
+        const bool k = i < m && keep(p0 + i);
+        const unsigned mask = __ballot_sync(0xffffffffu, k);
+        if (lane == 0) q.wcnt[warp] = __popc(mask);
+        __syncthreads();
+        int before = n, total = 0;
+        for (int w = 0; w < nwarps; ++w) {
+            const int c = q.wcnt[w];
+            if (w < warp) before += c;
+            total += c;
+        }
+        if (k) store(before + __popc(mask & ((1u << lane) - 1u)), p0 + i);
+        n += total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) q.n = n;
+    __syncthreads();
+}
+
 template <typename Queue, typename Keep, typename Work>
 __device__ __forceinline__ void ket_items(int nper, int j0, int64_t cnt, Queue& q, int& rot, Keep keep, Work work) {
-    const int lane = threadIdx.x & 31;
     for (int64_t base = 0; base < cnt; base += KQ_CAP) {
         const int m = static_cast<int>(cnt - base < KQ_CAP ? cnt - base : KQ_CAP);
-        if (threadIdx.x == 0) q.n = 0;
-        __syncthreads();
-        for (int i0 = 0; i0 < m; i0 += blockDim.x) {
-            const int i = i0 + threadIdx.x;
-            const int pos = j0 + static_cast<int>(base) + i;
-            const bool k = i < m && keep(pos);
-            const unsigned mask = __ballot_sync(0xffffffffu, k);
-            int w0 = 0;
-            if (lane == 0 && mask) w0 = atomicAdd(&q.n, __popc(mask));
-            w0 = __shfl_sync(0xffffffffu, w0, 0);
-            if (k) q.pos[w0 + __popc(mask & ((1u << lane) - 1u))] = pos;
-        }
-        __syncthreads();
+        compact(q, j0 + static_cast<int>(base), m, keep, [&](int slot, int pos) { q.pos[slot] = pos; });
         const int items = q.n * nper;
         int it = static_cast<int>(threadIdx.x) - rot;
         if (it < 0) it += blockDim.x;
@@ -522,6 +656,7 @@ __host__ __device__ constexpr size_t rsmem_bytes(int max_bra_prims, int max_ket_
 
 struct KetQueueR {
     int pos[KQ_CAP];
+    int wcnt[32];           // per-warp counts of one compaction step
     int pq[KQ_CAP + 1];     // exclusive prefix of primitive quartets over the chunk's entries
     int sc[KQ_CAP];         // sub-chunk of each entry
     int n;
@@ -570,23 +705,10 @@ __device__ __forceinline__ void ket_items_r(int nper, int j0, int64_t cnt, KetQu
     const int nbp = st.nbp;
     for (int64_t base = 0; base < cnt; base += KQ_CAP) {
         const int m = static_cast<int>(cnt - base < KQ_CAP ? cnt - base : KQ_CAP);
-        if (threadIdx.x == 0) q.n = 0;
-        __syncthreads();
-        for (int i0 = 0; i0 < m; i0 += blockDim.x) {
-            const int i = i0 + threadIdx.x;
-            const int pos = j0 + static_cast<int>(base) + i;
-            const bool k = i < m && keep(pos);
-            const unsigned mask = __ballot_sync(0xffffffffu, k);
-            int w0 = 0;
-            if (lane == 0 && mask) w0 = atomicAdd(&q.n, __popc(mask));
-            w0 = __shfl_sync(0xffffffffu, w0, 0);
-            if (k) {
-                const int slot = w0 + __popc(mask & ((1u << lane) - 1u));
-                q.pos[slot] = pos;
-                q.pq[slot] = qa.pv.npp[qa.sorted[pos]] * nbp;      // primitive quartets of the entry
-            }
-        }
-        __syncthreads();
+        compact(q, j0 + static_cast<int>(base), m, keep, [&](int slot, int pos) {
+            q.pos[slot] = pos;
+            q.pq[slot] = qa.pv.npp[qa.sorted[pos]] * nbp;          // primitive quartets of the entry
+        });
         const int ne = q.n;
         if (ne == 0) continue;                                      // uniform: q.n is shared
         // warp 0: exclusive prefix of the entries' primitive quartets and
@@ -651,7 +773,7 @@ __device__ __forceinline__ void ket_items_r(int nper, int j0, int64_t cnt, KetQu
 
 template <int CX, int CY, int NS, bool KGLOBAL, typename RT>
 __device__ __forceinline__ void jk_ket_class(const JKArgs& a, const BraStageT<RT>& st, int spos, double* Jt,
-                                             double* Ksm, KetQueueR& kq, int& rot, RT* Rbuf) {
+                                             facc* Ksm, KetQueueR& kq, int& rot, RT* Rbuf) {
     using Q = QClass<CX, CY>;
     const double q1 = a.q.sortedQ[spos];
     const double* bm = a.bmax;
@@ -736,8 +858,8 @@ __global__ void __launch_bounds__(JK_THREADS, AIMD_JK_MINB) jk_bra_kernel(JKArgs
     extern __shared__ double smem[];
     const int n = a.q.nao;
     const int krows = a.kglobal ? 0 : KK::KROWS;
-    double* Ksm = smem;
-    double* Jt = Ksm + (size_t)krows * n;
+    facc* Ksm = reinterpret_cast<facc*>(smem);
+    double* Jt = smem + (size_t)krows * n;
     RT* Rbuf = reinterpret_cast<RT*>(Jt + NS * KK::NROW * JK_THREADS);
     RT* Esm = Rbuf + a.rbuf;
     constexpr int yk = YK;
@@ -782,17 +904,17 @@ __global__ void __launch_bounds__(JK_THREADS, AIMD_JK_MINB) jk_bra_kernel(JKArgs
         const int kab = r / Q0::NAB, ab = r % Q0::NAB;
         const int ka = kab / st.nB, kb = kab % st.nB;
         const int m = st.oA + ka * Q0::NA + ab / Q0::NB, nb_ = st.oB + kb * Q0::NB + ab % Q0::NB;
-        atomicAdd(a.J + s * nn + (size_t)m * n + nb_, val);
+        fadd(a.J + s * nn + (size_t)m * n + nb_, val, __ldg(a.fix));
     }
     // flush K rows
     if (krows > 0) {
         constexpr int NFA = Q0::KA * Q0::NA;
         for (int i = threadIdx.x; i < krows * n; i += blockDim.x) {
-            const double val = Ksm[i];
-            if (val == 0.0) continue;
+            const facc val = Ksm[i];
+            if (val == 0) continue;
             const int col = i % n, f = (i / n) % KK::NF, s = i / (n * KK::NF);
             const int row = f < NFA ? st.oA + f : st.oB + (f - NFA);
-            atomicAdd(a.K + s * nn + (size_t)row * n + col, val);
+            atomicAdd(a.K + s * nn + (size_t)row * n + col, val);     // integer: order-independent
         }
     }
 }

@@ -25,7 +25,7 @@ struct GradArgs {
     int nx;
     double kfac;
     double thr;             // exact screening threshold on Q1 Q2 max|Gamma|
-    double* grad;           // [natm][3]
+    facc* grad;             // [natm][3] (fixed point, FIX_G)
     int natm;
     size_t rbuf;            // elements of the kernel's staged-R buffer (set per launch)
     const double* bmc;      // [nblock][nblock] max |Dc| per block pair
@@ -284,12 +284,14 @@ __device__ __forceinline__ void grad_prims_hoisted(const BraStageT<RT>& st, cons
     }
 }
 
-// Register footprint of the hoisted order (Gamma column, Y and the summed
-// ket step per contraction group), in bytes: used where it fits.
+// The hoisted order for the d-shell bra classes, where its register
+// footprint (Gamma column, Y and the summed ket step per contraction group)
+// fits; the per-primitive-quartet order for the others.
 template <int CX, int CY, typename RT>
 constexpr bool grad_hoist() {
     using Q = QClass<CX, CY>;
-    return sizeof(RT) * (Q::NROW * Q::KG + Q::KG * (Q::NHB + nherm(Q::LAB + 1))) <= 800;
+    // d-shell bras only (few bra primitives; see eri_column)
+    return CX >= 3 && sizeof(RT) * (Q::NROW * Q::KG + Q::KG * (Q::NHB + nherm(Q::LAB + 1))) <= 800;
 }
 
 // Gradient contribution of one column; adds A, B parts to gab and C, D
@@ -297,7 +299,7 @@ constexpr bool grad_hoist() {
 // of the ket pair's primitive quartets staged in Rs ([ik][ib][NH(L + 1)]).
 template <int CX, int CY, typename RT, bool RS = false>
 __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStageT<RT>& st, int P2, double QQ, int ic,
-                                            int id, int kg, double (&gab)[6], double* gsh,
+                                            int id, int kg, double (&gab)[6], facc* gsh,
                                             const RT* __restrict__ Rs = nullptr) {
     using Q = QClass<CX, CY>;
     using BE = BraE<Q::LA, Q::LB, 1>;
@@ -516,8 +518,8 @@ __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStageT<R
         const double da = dA[d], db = dB[d], dc = dC[d];
         gab[d] += da;
         gab[3 + d] += db;
-        atomicAdd(gsh + 3 * aC + d, dc);
-        atomicAdd(gsh + 3 * aD + d, -(da + db + dc));
+        fadd(gsh + 3 * aC + d, dc, FIX_G);
+        fadd(gsh + 3 * aD + d, -(da + db + dc), FIX_G);
     }
 }
 
@@ -525,17 +527,14 @@ __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStageT<R
 // block quartet, deg [|Dc|_AB |Dc|_CD + |k|/2 nx (|Dx|_AC |Dx|_BD +
 // |Dx|_AD |Dx|_BC)] >= max|Gamma|, can reach the threshold and the quartet
 // is not one-centre; the exact per-column test follows in grad_column.
-#ifndef AIMD_GRAD_RSMEM_MINL
-#define AIMD_GRAD_RSMEM_MINL 4
-#endif
 // Two-stage items (R_tuv to L + 1 staged per primitive quartet) for the
-// gradient of class pair (CX, CY).
+// gradient of class pair (CX, CY): the same classes as the J/K build.
 template <int CX, int CY>
-constexpr bool grad_rsmem() { return CY >= 1 && QClass<CX, CY>::L + 1 >= AIMD_GRAD_RSMEM_MINL; }
+constexpr bool grad_rsmem() { return QClass<CX, CY>::RSMEM; }
 
 template <int CX, int CY, typename RT>
 __device__ __forceinline__ void grad_ket_class(const GradArgs& a, const BraStageT<RT>& st, int spos, double (&gab)[6],
-                                               double* gsh, KetQueueR& kq, int& rot, RT* Rbuf) {
+                                               facc* gsh, KetQueueR& kq, int& rot, RT* Rbuf) {
     using Q = QClass<CX, CY>;
     constexpr bool RS = grad_rsmem<CX, CY>();
     const double q1 = a.q.sortedQ[spos];
@@ -585,7 +584,7 @@ template <int CX, int CY, typename RT>
 __global__ void __launch_bounds__(128, AIMD_GRAD_MINB) grad2e_bra_kernel(GradArgs a) {
     using Q0 = QClass<CX, 0>;
     extern __shared__ double smem[];
-    double* gsh = smem;
+    facc* gsh = reinterpret_cast<facc*>(smem);
     RT* Rbuf = reinterpret_cast<RT*>(smem + 3 * a.natm);
     RT* Esm = Rbuf + a.rbuf;
     __shared__ BraStageT<RT> st;
@@ -605,7 +604,7 @@ __global__ void __launch_bounds__(128, AIMD_GRAD_MINB) grad2e_bra_kernel(GradArg
     }
     __syncthreads();
     if (!any) return;
-    for (int i = threadIdx.x; i < 3 * a.natm; i += blockDim.x) gsh[i] = 0.0;
+    for (int i = threadIdx.x; i < 3 * a.natm; i += blockDim.x) gsh[i] = 0;
     stage_bra_e<Q0::LA, Q0::LB, 1>(st);
     __syncthreads();
     stage_bra_d<Q0::LA, Q0::LB>(st);
@@ -615,12 +614,12 @@ __global__ void __launch_bounds__(128, AIMD_GRAD_MINB) grad2e_bra_kernel(GradArg
     grad_ket_class<CX, CY, RT>(a, st, spos, gab, gsh, kq, rot, Rbuf);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        if (gab[d] != 0.0) atomicAdd(gsh + 3 * st.aA + d, gab[d]);
-        if (gab[3 + d] != 0.0) atomicAdd(gsh + 3 * st.aB + d, gab[3 + d]);
+        if (gab[d] != 0.0) fadd(gsh + 3 * st.aA + d, gab[d], FIX_G);
+        if (gab[3 + d] != 0.0) fadd(gsh + 3 * st.aB + d, gab[3 + d], FIX_G);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < 3 * a.natm; i += blockDim.x)
-        if (gsh[i] != 0.0) atomicAdd(a.grad + i, gsh[i]);
+        if (gsh[i] != 0) atomicAdd(a.grad + i, gsh[i]);
 }
 
 // Elements of the staged-R buffer of the (CX, CY) gradient kernel.

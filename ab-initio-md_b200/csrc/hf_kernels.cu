@@ -71,6 +71,7 @@ struct aimd_ctx {
     int64_t* counts_d;      // difference-density builds (threshold changes every call)
     double* bmax;           // [nblock][nblock] max |D| per block pair
     double* dmax;           // [1] max over bmax
+    double* jkfix;          // [1] fixed-point scale of the J/K accumulators
     double* bmc;            // gradient: [nblock][nblock] max |Dc| and max over x of |Dx|
     double* bmx;
     cudaStream_t cls_stream[NCLS];
@@ -85,6 +86,10 @@ struct aimd_ctx {
     void* cub_tmp;
     size_t cub_bytes;
     double* pos;            // [natm][3] device copy of the current geometry
+    // fixed-point accumulators (order-independent sums): J and K of one
+    // density, the nuclear gradient
+    facc *jacc = nullptr, *kacc = nullptr, *gacc = nullptr;
+    std::vector<double> charges_host;   // nuclear charges (host copy)
     // J/K: bra K rows in global memory for every class (otherwise only where
     // the shared rows would not fit); AIMD_JK_GLOBAL_K_ROWS=1 at creation
     int jk_global_rows = 0;
@@ -152,7 +157,11 @@ extern "C" int aimd_create(aimd_ctx** out, int natm, int nao, int nblock, const 
     CK(up_d(&c->sh_exp, sh_exp, nsprim));
     CK(up_d(&c->sh_coef, sh_coef, nsprim));
     CK(up_d(&c->charges, charges, natm));
+    c->charges_host.assign(charges, charges + natm);
     CK(dalloc(&c->pos, 3 * (size_t)natm));
+    CK(dalloc(&c->jacc, (size_t)nao * nao));
+    CK(dalloc(&c->kacc, (size_t)nao * nao));
+    CK(dalloc(&c->gacc, 3 * (size_t)natm));
     // shell pairs (si >= sj) grouped by class (l_i >= l_j after orientation)
     {
         std::vector<int> pi, pj;
@@ -227,6 +236,7 @@ extern "C" int aimd_create(aimd_ctx** out, int natm, int nao, int nblock, const 
         CK(dalloc(&c->counts_hi, (size_t)NSEG * (np + 1)));
         CK(dalloc(&c->bmax, (size_t)nblock * nblock));
         CK(dalloc(&c->dmax, 1));
+        CK(dalloc(&c->jkfix, 1));
         CK(dalloc(&c->bmc, (size_t)nblock * nblock));
         CK(dalloc(&c->bmx, (size_t)nblock * nblock));
         for (int cl = 0; cl < NCLS; ++cl) c->maxbp[cl] = 1;
@@ -253,7 +263,7 @@ extern "C" int aimd_destroy(aimd_ctx* c) {
                     c->sh_atom, c->sh_l, c->sh_ao, c->sh_p0, c->sh_np, c->sp_i, c->sp_j, c->sh_exp, c->sh_coef,
                     c->charges, c->pa, c->pb, c->npp, c->slot, c->rec, c->Q, c->by_class, c->idx_in,
                     c->tmp_idx, c->seg_id, c->seg_keys, c->seg_keys_out, c->seg_start, c->tmpQ, c->sortedQ,
-                    c->sorted, c->counts_jk, c->counts_g, c->counts_d, c->bmax, c->dmax, c->bmc, c->bmx, c->counts_hi, c->counts_hi_d, c->cub_tmp, c->pos};
+                    c->sorted, c->counts_jk, c->counts_g, c->counts_d, c->bmax, c->dmax, c->jkfix, c->bmc, c->bmx, c->counts_hi, c->counts_hi_d, c->cub_tmp, c->pos, c->jacc, c->kacc, c->gacc};
     for (void* p : ptrs) cudaFree(p);
     for (int i = 0; i < NCLS; ++i) {
         if (c->cls_stream[i]) cudaStreamDestroy(c->cls_stream[i]);
@@ -400,7 +410,22 @@ __global__ void block_dmax_kernel(int nblock, int nao, int nset, const int* blk_
     bmax[i] = m;
 }
 
-__global__ void max_reduce_kernel(int n, const double* x, double* out) {
+// out = acc / scale (add = 0) or out += acc / scale (add = 1); the scale is
+// *scale_p when that is given (a device scalar), else scale
+__global__ void from_fixed_kernel(size_t n, const facc* acc, const double* scale_p, double scale, double* out,
+                                  int add) {
+    const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double v = from_fixed(acc[i], scale_p ? *scale_p : scale);
+    out[i] = add ? out[i] + v : v;
+}
+void from_fixed(cudaStream_t st, size_t n, const facc* acc, const double* scale_p, double scale, double* out,
+                int add) {
+    from_fixed_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, acc, scale_p, scale, out, add);
+}
+
+// *out = max of x[0 .. n); fix (optional) = jk_fix_for(*out)
+__global__ void max_reduce_kernel(int n, const double* x, double* out, double* fix) {
     __shared__ double sm[256];
     double m = 0.0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, x[i]);
@@ -410,7 +435,10 @@ __global__ void max_reduce_kernel(int n, const double* x, double* out) {
         if (threadIdx.x < w) sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + w]);
         __syncthreads();
     }
-    if (threadIdx.x == 0) *out = sm[0];
+    if (threadIdx.x == 0) {
+        *out = sm[0];
+        if (fix) *fix = jk_fix_for(sm[0]);
+    }
 }
 
 PairView pair_view(aimd_ctx* c) { return PairView{c->pa, c->pb, c->slot, c->npp, c->rec}; }
@@ -625,8 +653,13 @@ extern "C" int aimd_jk(aimd_ctx* c, int nset, const double* D, double* J, double
     if (int r = hi_counts(c, st, &hi)) return r;
     const bool mixed = hi != nullptr;
     const size_t nn = (size_t)c->nao * c->nao;
-    CK(cudaMemsetAsync(J, 0, sizeof(double) * nset * nn, st));
-    CK(cudaMemsetAsync(K, 0, sizeof(double) * nset * nn, st));
+    // fixed-point scale of the accumulators from max |D| over the sets
+    const int nb2 = c->nblock * c->nblock;
+    block_dmax_kernel<<<(nb2 + 127) / 128, 128, 0, st>>>(c->nblock, c->nao, nset, c->blk_l, c->blk_ncon, c->blk_ao, D,
+                                                         c->bmax);
+    max_reduce_kernel<<<1, 256, 0, st>>>(nb2, c->bmax, c->dmax, c->jkfix);
+    c->launches += 2;
+
     // one pass per density (UHF: alpha and beta)
     const LaunchEnv e = launch_env(c);
     for (int s0 = 0; s0 < nset; ++s0) {
@@ -634,8 +667,11 @@ extern "C" int aimd_jk(aimd_ctx* c, int nset, const double* D, double* J, double
         a.q = quartet_args(c, c->counts_jk);
         a.q.counts_hi = hi;
         a.D = D + s0 * nn;
-        a.J = J + s0 * nn;
-        a.K = K + s0 * nn;
+        a.J = c->jacc;
+        a.K = c->kacc;
+        a.fix = c->jkfix;
+        CK(cudaMemsetAsync(c->jacc, 0, sizeof(facc) * nn, st));
+        CK(cudaMemsetAsync(c->kacc, 0, sizeof(facc) * nn, st));
         a.bmax = nullptr;
         a.nblock = c->nblock;
         a.dthr = 0.0;
@@ -646,6 +682,10 @@ extern "C" int aimd_jk(aimd_ctx* c, int nset, const double* D, double* J, double
         AIMD_EACH_CLASS_CONCURRENT(AIMD_JK, "aimd_jk", AIMD_NL);
 #undef AIMD_NL
 #undef AIMD_JK
+        from_fixed(st, nn, c->jacc, c->jkfix, 0.0, J + s0 * nn, 0);
+        from_fixed(st, nn, c->kacc, c->jkfix, 0.0, K + s0 * nn, 0);
+        c->launches += 2;
+        CK(cudaGetLastError());
     }
     return AIMD_OK;
 }
@@ -680,7 +720,7 @@ extern "C" int aimd_jk_delta(aimd_ctx* c, int nset, const double* D, double* J, 
     const int nb2 = c->nblock * c->nblock;
     block_dmax_kernel<<<(nb2 + 127) / 128, 128, 0, st>>>(c->nblock, c->nao, nset, c->blk_l, c->blk_ncon, c->blk_ao, D,
                                                          c->bmax);
-    max_reduce_kernel<<<1, 256, 0, st>>>(nb2, c->bmax, c->dmax);
+    max_reduce_kernel<<<1, 256, 0, st>>>(nb2, c->bmax, c->dmax, c->jkfix);
     c->launches += 2;
     CK(cudaGetLastError());
     // enumerate at max(thr, dthr / max|D|): the integral screen still holds,
@@ -695,16 +735,18 @@ extern "C" int aimd_jk_delta(aimd_ctx* c, int nset, const double* D, double* J, 
         hi = c->counts_hi_d;
     }
     const bool mixed = hi != nullptr;
-    CK(cudaMemsetAsync(J, 0, sizeof(double) * nset * nn, st));
-    CK(cudaMemsetAsync(K, 0, sizeof(double) * nset * nn, st));
+
     const LaunchEnv e = launch_env(c);
     for (int s0 = 0; s0 < nset; ++s0) {
         JKArgs a;
         a.q = quartet_args(c, c->counts_d);
         a.q.counts_hi = hi;
         a.D = D + s0 * nn;
-        a.J = J + s0 * nn;
-        a.K = K + s0 * nn;
+        a.J = c->jacc;
+        a.K = c->kacc;
+        a.fix = c->jkfix;
+        CK(cudaMemsetAsync(c->jacc, 0, sizeof(facc) * nn, st));
+        CK(cudaMemsetAsync(c->kacc, 0, sizeof(facc) * nn, st));
         a.bmax = c->bmax;
         a.nblock = c->nblock;
         a.dthr = dthr;
@@ -715,6 +757,10 @@ extern "C" int aimd_jk_delta(aimd_ctx* c, int nset, const double* D, double* J, 
         AIMD_EACH_CLASS_CONCURRENT(AIMD_JK, "aimd_jk_delta", AIMD_NL);
 #undef AIMD_NL
 #undef AIMD_JK
+        from_fixed(st, nn, c->jacc, c->jkfix, 0.0, J + s0 * nn, 0);
+        from_fixed(st, nn, c->kacc, c->jkfix, 0.0, K + s0 * nn, 0);
+        c->launches += 2;
+        CK(cudaGetLastError());
     }
     return AIMD_OK;
 }
@@ -847,7 +893,7 @@ extern "C" int aimd_grad2e(aimd_ctx* c, const double* Dc, int nx, const double* 
         if (int r = build_counts(c, thr_enum, c->counts_g, st)) return r;
         c->thr_g = thr_enum;
     }
-    CK(cudaMemsetAsync(grad, 0, sizeof(double) * 3 * c->natm, st));
+    CK(cudaMemsetAsync(c->gacc, 0, sizeof(facc) * 3 * c->natm, st));
     const int nb2 = c->nblock * c->nblock;
     block_dmax_kernel<<<(nb2 + 127) / 128, 128, 0, st>>>(c->nblock, c->nao, 1, c->blk_l, c->blk_ncon, c->blk_ao, Dc,
                                                          c->bmc);
@@ -869,7 +915,7 @@ extern "C" int aimd_grad2e(aimd_ctx* c, const double* Dc, int nx, const double* 
     a.nx = nx;
     a.kfac = kfac;
     a.thr = thr;
-    a.grad = grad;
+    a.grad = c->gacc;
     a.natm = c->natm;
     a.rbuf = 0;
     a.bmc = c->bmc;
@@ -881,6 +927,9 @@ extern "C" int aimd_grad2e(aimd_ctx* c, const double* Dc, int nx, const double* 
     AIMD_EACH_CLASS_CONCURRENT(AIMD_GRAD, "aimd_grad2e", AIMD_NL);
 #undef AIMD_NL
 #undef AIMD_GRAD
+    from_fixed(st, 3 * (size_t)c->natm, c->gacc, nullptr, FIX_G, grad, 0);
+    ++c->launches;
+    CK(cudaGetLastError());
     return AIMD_OK;
 }
 
@@ -919,8 +968,14 @@ extern "C" int aimd_onee(aimd_ctx* c, const double* origin, double* S, double* T
 extern "C" int aimd_onee_grad(aimd_ctx* c, const double* W, const double* D, double* grad, void* stream) {
     if (!c || !W || !D || !grad || !c->have_geometry) return AIMD_ERR_ARG;
     int n = 0;
-    cudaError_t r = launch_onee_grad(launch_env(c), shell_view(c), c->sp_cls_start, W, D, grad,
-                                     static_cast<cudaStream_t>(stream), &n);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    CK(cudaMemsetAsync(c->gacc, 0, sizeof(facc) * 3 * c->natm, st));
+    cudaError_t r = launch_onee_grad(launch_env(c), shell_view(c), c->sp_cls_start, W, D, c->gacc, st, &n);
+    if (r == cudaSuccess) {
+        from_fixed(st, 3 * (size_t)c->natm, c->gacc, nullptr, FIX_G, grad, 1);
+        ++n;
+        r = cudaGetLastError();
+    }
     c->launches += n;
     if (r == cudaErrorInvalidConfiguration) {
         snprintf(g_err, sizeof g_err, "aimd_onee_grad: too many atoms for the shared accumulator");
@@ -961,5 +1016,31 @@ extern "C" int aimd_pair_data(aimd_ctx* c, int* npp_host, int* cls_host, int* so
 }
 
 extern "C" uint64_t aimd_launch_count(aimd_ctx* c) { return c ? c->launches : 0; }
+
+extern "C" int aimd_sizes(aimd_ctx* c, int* natm, int* nao) {
+    if (!c || !natm || !nao) return AIMD_ERR_ARG;
+    *natm = c->natm;
+    *nao = c->nao;
+    return AIMD_OK;
+}
+
+// sum_{A<B} Z_A Z_B / |R_A - R_B| of the current geometry (host value; the
+// positions are read back on `stream`, after the aimd_set_geometry that set
+// them)
+extern "C" int aimd_nuclear_repulsion(aimd_ctx* c, double* energy, void* stream) {
+    if (!c || !energy || !c->have_geometry) return AIMD_ERR_ARG;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    std::vector<double> x(3 * (size_t)c->natm);
+    CK(cudaMemcpyAsync(x.data(), c->pos, sizeof(double) * x.size(), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    double e = 0.0;
+    for (int a = 0; a < c->natm; ++a)
+        for (int b = 0; b < a; ++b) {
+            const double dx = x[3 * a] - x[3 * b], dy = x[3 * a + 1] - x[3 * b + 1], dz = x[3 * a + 2] - x[3 * b + 2];
+            e += c->charges_host[a] * c->charges_host[b] / sqrt(dx * dx + dy * dy + dz * dz);
+        }
+    *energy = e;
+    return AIMD_OK;
+}
 
 extern "C" int aimd_version(void) { return AIMD_ABI_VERSION; }

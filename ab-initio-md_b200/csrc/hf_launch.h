@@ -48,7 +48,7 @@ AIMD_DECLARE_CLASS(5)
 cudaError_t launch_onee(const LaunchEnv& e, const ShellView& sv, const int* sp_cls_start, const double* origin,
                         double* S, double* T, double* M, double* V, cudaStream_t st, int* nlaunch);
 cudaError_t launch_onee_grad(const LaunchEnv& e, const ShellView& sv, const int* sp_cls_start, const double* W,
-                             const double* D, double* grad, cudaStream_t st, int* nlaunch);
+                             const double* D, facc* grad, cudaStream_t st, int* nlaunch);
 
 constexpr size_t kSmemLimit = 227 * 1024;     // dynamic shared memory per CTA (sm_100a)
 

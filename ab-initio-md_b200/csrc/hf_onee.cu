@@ -20,8 +20,8 @@ cudaError_t launch_onee(const LaunchEnv& e, const ShellView& sv, const int* sp_c
     return cudaGetLastError();
 }
 
-cudaError_t launch_onee_grad(const LaunchEnv& e, const ShellView& sv, const int* sp_cls_start, const double* W, const double* D, double* grad, cudaStream_t st, int* nlaunch) {
-    const size_t smem = sizeof(double) * 3 * e.natm;
+cudaError_t launch_onee_grad(const LaunchEnv& e, const ShellView& sv, const int* sp_cls_start, const double* W, const double* D, facc* grad, cudaStream_t st, int* nlaunch) {
+    const size_t smem = sizeof(facc) * 3 * e.natm;
     if (smem > 48 * 1024) return cudaErrorInvalidConfiguration;
 #define AIMD_LAUNCH_1G(CL)                                                                                    \
     {                                                                                                         \

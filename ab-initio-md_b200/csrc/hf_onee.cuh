@@ -134,9 +134,9 @@ __global__ void __launch_bounds__(128) onee_kernel(ShellView sv, int p_begin, in
 // d/dR sum D V for shell pairs of class (LI, LJ); block-shared accumulator.
 template <int LI, int LJ>
 __global__ void __launch_bounds__(128) onee_grad_kernel(ShellView sv, int p_begin, int p_end,
-                                                        const double* W, const double* Dm, double* grad) {
-    extern __shared__ double gsh[];
-    for (int i = threadIdx.x; i < 3 * sv.natm; i += blockDim.x) gsh[i] = 0.0;
+                                                        const double* W, const double* Dm, facc* grad) {
+    extern __shared__ facc gsh[];
+    for (int i = threadIdx.x; i < 3 * sv.natm; i += blockDim.x) gsh[i] = 0;
     __syncthreads();
     const int ip = p_begin + blockIdx.x * blockDim.x + threadIdx.x;
     if (ip < p_end) {
@@ -264,20 +264,20 @@ __global__ void __launch_bounds__(128) onee_grad_kernel(ShellView sv, int p_begi
                         gc[d] *= pref;
                         gNA[d] += ga[d];
                         gNB[d] -= ga[d] + gc[d];
-                        atomicAdd(&gsh[3 * c + d], gc[d]);
+                        fadd(&gsh[3 * c + d], gc[d], FIX_G);
                     }
                 }
             }
         }
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-            atomicAdd(&gsh[3 * ai + d], gA[d] + gNA[d]);
-            atomicAdd(&gsh[3 * aj + d], -gA[d] + gNB[d]);
+            fadd(&gsh[3 * ai + d], gA[d] + gNA[d], FIX_G);
+            fadd(&gsh[3 * aj + d], -gA[d] + gNB[d], FIX_G);
         }
     }
     __syncthreads();
     for (int i = threadIdx.x; i < 3 * sv.natm; i += blockDim.x)
-        if (gsh[i] != 0.0) atomicAdd(&grad[i], gsh[i]);
+        if (gsh[i] != 0) atomicAdd(&grad[i], gsh[i]);
 }
 
 }  // namespace hf

@@ -129,6 +129,14 @@ int aimd_onee_grad(aimd_ctx *ctx, const double *W, const double *D, double *grad
 int aimd_quartet_counts(aimd_ctx *ctx, int which, int64_t *out_host);
 int aimd_pair_data(aimd_ctx *ctx, int *npp_host, int *cls_host, int *sorted_host);
 
+/* Sizes of the context's basis: atoms and AOs. */
+int aimd_sizes(aimd_ctx *ctx, int *natm, int *nao);
+
+/* Nuclear repulsion sum_{A<B} Z_A Z_B / R_AB of the current geometry into
+ * *energy (host); reads the positions back on `stream` and waits for it.
+ * aimd/qc/integrals.py:1421-1426 (nuclear_repulsion_energy). */
+int aimd_nuclear_repulsion(aimd_ctx *ctx, double *energy, void *stream);
+
 uint64_t aimd_launch_count(aimd_ctx *ctx);
 const char *aimd_last_error(void);
 int aimd_version(void);
