@@ -35,9 +35,11 @@ cudaError_t AIMD_GRAD_NAME(const LaunchEnv& e, const GradArgs& a0, cudaStream_t 
     GradArgs a = a0;
     a.rbuf = grad_rbuf_elems<CX, CY, RT>(e.maxbp[CX], e.maxbp[CY]);
     const size_t smem = grad_smem_bytes<CX, RT>(e.natm, e.maxbp[CX], a.rbuf);
-    cudaError_t r = set_smem_limit((const void*)grad2e_bra_kernel<CX, CY, RT>, smem);
+    const void* kernel = (const void*)grad2e_bra_kernel<CX, CY, RT>;
+    cudaError_t r = set_smem_limit(kernel, smem);
     if (r != cudaSuccess) return r;
-    grad2e_bra_kernel<CX, CY, RT><<<cnt, 128, smem, st>>>(a);
+    a.plan = e.plan_of(CX, CY, sizeof(RT) == sizeof(double) ? 0 : 1);
+    grad2e_bra_kernel<CX, CY, RT><<<persistent_grid(kernel, 128, smem, e.nsm), 128, smem, st>>>(a);
     return cudaGetLastError();
 }
 

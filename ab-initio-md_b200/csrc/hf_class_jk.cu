@@ -49,9 +49,11 @@ cudaError_t launch_one(const LaunchEnv& e, const JKArgs& a0, cudaStream_t st) {
         a.kglobal = 1;
         smem = jk_smem_bytes<CX, 1, RT>(e.nao, e.maxbp[CX], a.rbuf, true);
     }
-    cudaError_t r = set_smem_limit((const void*)jk_bra_kernel<CX, 1, RT, YK>, smem);
+    const void* kernel = (const void*)jk_bra_kernel<CX, 1, RT, YK>;
+    cudaError_t r = set_smem_limit(kernel, smem);
     if (r != cudaSuccess) return r;
-    jk_bra_kernel<CX, 1, RT, YK><<<e.cls_count[CX], JK_THREADS, smem, st>>>(a);
+    a.plan = e.plan_of(CX, YK < 0 ? 0 : YK, sizeof(RT) == sizeof(double) ? 0 : 1);
+    jk_bra_kernel<CX, 1, RT, YK><<<persistent_grid(kernel, JK_THREADS, smem, e.nsm), JK_THREADS, smem, st>>>(a);
     return cudaGetLastError();
 }
 }  // namespace

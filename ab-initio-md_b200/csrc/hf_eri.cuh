@@ -423,6 +423,78 @@ __device__ __forceinline__ void ket_range(const QuartetArgs& a, int seg, int spo
     }
 }
 
+// ---------------------------------------------------------------- work plan
+// The class kernels are persistent: their CTAs take chunks of (bra pair,
+// ket window) from a device counter until the launch's plan is used up, so
+// that the few heavy bras (many primitives, long ket lists) are spread over
+// many CTAs instead of setting the kernel's duration. A plan holds, per bra
+// of the class, the exclusive prefix of its chunk counts; chunk j of nch
+// covers the bra's work units [W j / nch, W (j + 1) / nch) in ket segment
+// order. Work of a ket pair of segment sub: bra primitive pairs x twice
+// the segment's typical ket primitive pairs x the column items per pair.
+struct WorkPlan {
+    const int* off;     // [nbra + 1] chunk prefix over the bras of the class (off[nbra]: chunks)
+    int* next;          // chunk counter of the launch (zeroed with the plan)
+};
+
+__host__ __device__ constexpr int ket_prims2(int ppb) {
+    return ppb == 0 ? 2 : ppb == 1 ? 5 : ppb == 2 ? 11 : ppb == 3 ? 23 : ppb == 4 ? 47 : 80;
+}
+
+template <int CX, int CY>
+__device__ __forceinline__ int64_t ket_work(int sub);
+
+// Work units of bra position spos against ket class CY in the ket ranges
+// that the kernels of type RT evaluate.
+template <int CX, int CY, typename RT>
+__device__ int64_t bra_work(const QuartetArgs& q, int spos) {
+    int64_t w = 0;
+    for (int sub = 0; sub < NSUB; ++sub) {
+        int64_t kb, ke;
+        ket_range<RT>(q, CY * NSUB + sub, spos, kb, ke);
+        if (ke > kb) w += (ke - kb) * ket_work<CX, CY>(sub);
+    }
+    return w * q.pv.npp[q.sorted[spos]];
+}
+
+// Kets [k0, k1) of a segment of len kets, each of weight wk, whose work
+// starts inside the window [w0, w1) (acc: work of the segments before).
+__device__ __forceinline__ void window_kets(int64_t w0, int64_t w1, int64_t acc, int64_t wk, int64_t len,
+                                            int64_t& k0, int64_t& k1) {
+    auto first = [&](int64_t x) { return x <= 0 ? int64_t(0) : ((x + wk - 1) / wk < len ? (x + wk - 1) / wk : len); };
+    k0 = first(w0 - acc);
+    k1 = first(w1 - acc);
+}
+
+// Chunk j of nch of a bra of W work units: [W j / nch, W (j + 1) / nch),
+// without forming W j.
+__device__ __forceinline__ int64_t chunk_edge(int64_t W, int j, int nch) {
+    const int64_t q = W / nch, r = W % nch;
+    return q * j + (r * j) / nch;
+}
+
+// The next chunk of the launch for this CTA: thread 0 takes it from the
+// counter and finds its bra (last b with off[b] <= c); all threads return
+// the same (c, b) and c >= off[nbra] when the plan is used up.
+__device__ __forceinline__ void next_chunk(const WorkPlan& plan, int nbra, int* sh, int& c, int& b) {
+    if (threadIdx.x == 0) {
+        const int cc = atomicAdd(plan.next, 1);
+        int lo = 0, hi = nbra;                          // off[lo] <= cc < off[hi] while cc < total
+        if (cc < plan.off[nbra]) {
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (plan.off[mid] <= cc) lo = mid;
+                else hi = mid;
+            }
+        }
+        sh[0] = cc;
+        sh[1] = lo;
+    }
+    __syncthreads();
+    c = sh[0];
+    b = sh[1];
+}
+
 template <typename RT>
 __device__ __forceinline__ void load_stage(const QuartetArgs& a, int P1, BraStageT<RT>& st, RT* E) {
     st.P1 = P1;
@@ -455,6 +527,7 @@ struct JKArgs {
     // 1: the K rows of the bra functions accumulate in global memory (set per
     // launch when the per-CTA shared rows, NF x nao doubles, would not fit)
     int kglobal;
+    WorkPlan plan;      // chunks of the launch (set per launch)
 };
 
 // Digest one column (fixed ket component pair cd, all ket contractions kk)
@@ -579,6 +652,12 @@ __device__ __forceinline__ int seg_groups(int sub) {
     const int g = (ncs + KG - 1) / KG;
     return g < NKG ? g : NKG;
 }
+template <int CX, int CY>
+__device__ __forceinline__ int64_t ket_work(int sub) {
+    using Q = QClass<CX, CY>;
+    return (int64_t)ket_prims2(sub / NCONB) * Q::NCD * seg_groups<Q::KG, Q::NKG>(sub);
+}
+
 struct KetQueue {
     int pos[KQ_CAP];
     int wcnt[32];           // per-warp counts of one compaction step
@@ -771,18 +850,27 @@ __device__ __forceinline__ void ket_items_r(int nper, int j0, int64_t cnt, KetQu
     }
 }
 
+// The ket pairs of class CY for bra position spos whose work falls in the
+// chunk's window [w0, w1).
 template <int CX, int CY, int NS, bool KGLOBAL, typename RT>
 __device__ __forceinline__ void jk_ket_class(const JKArgs& a, const BraStageT<RT>& st, int spos, double* Jt,
-                                             facc* Ksm, KetQueueR& kq, int& rot, RT* Rbuf) {
+                                             facc* Ksm, KetQueueR& kq, int& rot, RT* Rbuf, int64_t w0,
+                                             int64_t w1) {
     using Q = QClass<CX, CY>;
     const double q1 = a.q.sortedQ[spos];
     const double* bm = a.bmax;
     const int nb = a.nblock;
+    int64_t acc = 0;
     for (int sub = 0; sub < NSUB; ++sub) {
         const int seg = CY * NSUB + sub;
         int64_t kb, ke;
         ket_range<RT>(a.q, seg, spos, kb, ke);
         if (ke <= kb) continue;
+        const int64_t wk = ket_work<CX, CY>(sub) * st.nbp;
+        int64_t k0, k1;
+        window_kets(w0, w1, acc, wk, ke - kb, k0, k1);
+        acc += (ke - kb) * wk;
+        if (k1 <= k0) continue;
         // difference densities: density-weighted test on the six block pairs
         auto keep = [&](int pos) {
             if (!bm) return true;
@@ -815,11 +903,11 @@ __device__ __forceinline__ void jk_ket_class(const JKArgs& a, const BraStageT<RT
                 jk_digest_column<CX, CY, NS, KGLOBAL>(a, st, P2, C, Dd, ic, id, kg, vd, Jt, Ksm);
             }
         };
-        const int j0 = a.q.seg_start[seg] + static_cast<int>(kb);
+        const int j0 = a.q.seg_start[seg] + static_cast<int>(kb + k0);
         if constexpr (Q::RSMEM) {
-            ket_items_r<Q::L>(Q::NCD * nkg, j0, ke - kb, kq, rot, st, a.q, Rbuf, keep, work);
+            ket_items_r<Q::L>(Q::NCD * nkg, j0, k1 - k0, kq, rot, st, a.q, Rbuf, keep, work);
         } else {
-            ket_items(Q::NCD * nkg, j0, ke - kb, kq, rot, keep,
+            ket_items(Q::NCD * nkg, j0, k1 - k0, kq, rot, keep,
                       [&](int pos, int r) { work(pos, r, static_cast<const RT*>(nullptr)); });
         }
     }
@@ -831,10 +919,9 @@ struct JKKernel {
     static constexpr int NROW = Q0::NROW;
     static constexpr int NF = Q0::KA * Q0::NA + Q0::KB * Q0::NB;
     static constexpr int ESIZE = BraE<Q0::LA, Q0::LB, 0>::SIZE;
-    // bra classes above ss: one kernel per ket class (one CTA per bra pair
-    // each): shorter CTAs that fill the machine, and each kernel holds the
-    // code of one ket class only, so the CTAs resident on an SM share their
-    // instructions; dd bras accumulate K in global memory
+    // bra classes above ss: one kernel per ket class, so that each kernel
+    // holds the code of one ket class only and the CTAs resident on an SM
+    // share their instructions; dd bras accumulate K in global memory
     static constexpr bool SPLIT = CX >= 1;
     static constexpr int NY = SPLIT ? CX + 1 : 1;
     static constexpr bool KGLOBAL = CX == 5;
@@ -847,7 +934,8 @@ constexpr int JK_THREADS = 128;
 
 // RT = double: the FP64 quartets; RT = float: the FP32 quartets of the
 // mixed-precision path (their J/K contributions still accumulate in FP64).
-// YK = ket class of this kernel, or -1: every ket class in each CTA.
+// YK = ket class of this kernel (-1: the ss bras, whose only ket class is ss).
+// Persistent: a CTA runs chunks of the launch's work plan until it is used up.
 #ifndef AIMD_JK_MINB
 #define AIMD_JK_MINB 1
 #endif
@@ -855,67 +943,60 @@ template <int CX, int NS, typename RT, int YK>
 __global__ void __launch_bounds__(JK_THREADS, AIMD_JK_MINB) jk_bra_kernel(JKArgs a) {
     using KK = JKKernel<CX, NS>;
     using Q0 = QClass<CX, 0>;
+    constexpr int Y = YK < 0 ? 0 : YK;      // the unsplit kernel (CX = 0) has one ket class too
+    static_assert(YK >= 0 || CX == 0, "bra classes above ss are split by ket class");
     extern __shared__ double smem[];
     const int n = a.q.nao;
+    const size_t nn = (size_t)n * n;
     const int krows = a.kglobal ? 0 : KK::KROWS;
     facc* Ksm = reinterpret_cast<facc*>(smem);
     double* Jt = smem + (size_t)krows * n;
     RT* Rbuf = reinterpret_cast<RT*>(Jt + NS * KK::NROW * JK_THREADS);
     RT* Esm = Rbuf + a.rbuf;
-    constexpr int yk = YK;
-    const int spos = a.q.cls_start[CX] + (int)blockIdx.x;
-    const int P1 = a.q.sorted[spos];
     __shared__ BraStageT<RT> st;
     __shared__ KetQueueR kq;
-    __shared__ int any;
-    if (threadIdx.x == 0) {
-        load_stage(a.q, P1, st, Esm);
-        int64_t tot = 0;
-        for (int y = 0; y <= CX; ++y)
-            if (yk < 0 || y == yk)
-                for (int sub = 0; sub < NSUB; ++sub) {
-                    int64_t kb, ke;
-                    ket_range<RT>(a.q, y * NSUB + sub, spos, kb, ke);
-                    tot += ke > kb ? ke - kb : 0;
-                }
-        any = tot > 0;
-    }
-    __syncthreads();
-    if (!any) return;
-    for (int i = threadIdx.x; i < krows * n + NS * KK::NROW * JK_THREADS; i += blockDim.x) smem[i] = 0.0;
-    stage_bra_e<Q0::LA, Q0::LB, 0>(st);
-    __syncthreads();
-    constexpr bool KG_ = KK::KGLOBAL;
-    int rot = 0;
-    if constexpr (yk < 0 || yk == 0) jk_ket_class<CX, 0, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot, Rbuf);
-    if constexpr (CX >= 1 && (yk < 0 || yk == 1)) jk_ket_class<CX, 1, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot, Rbuf);
-    if constexpr (CX >= 2 && (yk < 0 || yk == 2)) jk_ket_class<CX, 2, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot, Rbuf);
-    if constexpr (CX >= 3 && (yk < 0 || yk == 3)) jk_ket_class<CX, 3, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot, Rbuf);
-    if constexpr (CX >= 4 && (yk < 0 || yk == 4)) jk_ket_class<CX, 4, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot, Rbuf);
-    if constexpr (CX >= 5 && (yk < 0 || yk == 5)) jk_ket_class<CX, 5, NS, KG_, RT>(a, st, spos, Jt, Ksm, kq, rot, Rbuf);
-    __syncthreads();
-    const size_t nn = (size_t)n * n;
-    // flush J_ab: one thread per (set, row) sums the per-thread slots
-    for (int i = threadIdx.x; i < NS * KK::NROW; i += blockDim.x) {
-        double val = 0.0;
-        for (int t = 0; t < JK_THREADS; ++t) val += Jt[i * JK_THREADS + t];
-        if (val == 0.0) continue;
-        const int s = i / KK::NROW, r = i % KK::NROW;
-        const int kab = r / Q0::NAB, ab = r % Q0::NAB;
-        const int ka = kab / st.nB, kb = kab % st.nB;
-        const int m = st.oA + ka * Q0::NA + ab / Q0::NB, nb_ = st.oB + kb * Q0::NB + ab % Q0::NB;
-        fadd(a.J + s * nn + (size_t)m * n + nb_, val, __ldg(a.fix));
-    }
-    // flush K rows
-    if (krows > 0) {
-        constexpr int NFA = Q0::KA * Q0::NA;
-        for (int i = threadIdx.x; i < krows * n; i += blockDim.x) {
-            const facc val = Ksm[i];
-            if (val == 0) continue;
-            const int col = i % n, f = (i / n) % KK::NF, s = i / (n * KK::NF);
-            const int row = f < NFA ? st.oA + f : st.oB + (f - NFA);
-            atomicAdd(a.K + s * nn + (size_t)row * n + col, val);     // integer: order-independent
+    __shared__ int sh[2];
+    const int nbra = a.q.cls_start[CX + 1] - a.q.cls_start[CX];
+    const int total = a.plan.off[nbra];
+    for (;;) {
+        int c, b;
+        next_chunk(a.plan, nbra, sh, c, b);
+        if (c >= total) break;                                  // uniform: c is shared
+        const int spos = a.q.cls_start[CX] + b;
+        const int nch = a.plan.off[b + 1] - a.plan.off[b], j = c - a.plan.off[b];
+        const int64_t W = bra_work<CX, Y, RT>(a.q, spos);
+        if (threadIdx.x == 0) load_stage(a.q, a.q.sorted[spos], st, Esm);
+        for (int i = threadIdx.x; i < krows * n + NS * KK::NROW * JK_THREADS; i += blockDim.x) smem[i] = 0.0;
+        __syncthreads();
+        stage_bra_e<Q0::LA, Q0::LB, 0>(st);
+        __syncthreads();
+        int rot = 0;
+        jk_ket_class<CX, Y, NS, KK::KGLOBAL, RT>(a, st, spos, Jt, Ksm, kq, rot, Rbuf, chunk_edge(W, j, nch),
+                                                 chunk_edge(W, j + 1, nch));
+        __syncthreads();
+        // flush J_ab: one thread per (set, row) sums the per-thread slots
+        for (int i = threadIdx.x; i < NS * KK::NROW; i += blockDim.x) {
+            double val = 0.0;
+            for (int t = 0; t < JK_THREADS; ++t) val += Jt[i * JK_THREADS + t];
+            if (val == 0.0) continue;
+            const int s = i / KK::NROW, r = i % KK::NROW;
+            const int kab = r / Q0::NAB, ab = r % Q0::NAB;
+            const int ka = kab / st.nB, kb = kab % st.nB;
+            const int m = st.oA + ka * Q0::NA + ab / Q0::NB, nb_ = st.oB + kb * Q0::NB + ab % Q0::NB;
+            fadd(a.J + s * nn + (size_t)m * n + nb_, val, __ldg(a.fix));
         }
+        // flush K rows
+        if (krows > 0) {
+            constexpr int NFA = Q0::KA * Q0::NA;
+            for (int i = threadIdx.x; i < krows * n; i += blockDim.x) {
+                const facc val = Ksm[i];
+                if (val == 0) continue;
+                const int col = i % n, f = (i / n) % KK::NF, s = i / (n * KK::NF);
+                const int row = f < NFA ? st.oA + f : st.oB + (f - NFA);
+                atomicAdd(a.K + s * nn + (size_t)row * n + col, val);     // integer: order-independent
+            }
+        }
+        __syncthreads();
     }
 }
 

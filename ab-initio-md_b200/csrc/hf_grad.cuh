@@ -31,6 +31,7 @@ struct GradArgs {
     const double* bmc;      // [nblock][nblock] max |Dc| per block pair
     const double* bmx;      // [nblock][nblock] max over x of |Dx| per block pair (nx > 0)
     int nblock;
+    WorkPlan plan;          // chunks of the launch (set per launch)
 };
 
 // Bra derivative coefficients of one primitive pair, per direction d:
@@ -534,17 +535,24 @@ constexpr bool grad_rsmem() { return QClass<CX, CY>::RSMEM; }
 
 template <int CX, int CY, typename RT>
 __device__ __forceinline__ void grad_ket_class(const GradArgs& a, const BraStageT<RT>& st, int spos, double (&gab)[6],
-                                               facc* gsh, KetQueueR& kq, int& rot, RT* Rbuf) {
+                                               facc* gsh, KetQueueR& kq, int& rot, RT* Rbuf, int64_t w0,
+                                               int64_t w1) {
     using Q = QClass<CX, CY>;
     constexpr bool RS = grad_rsmem<CX, CY>();
     const double q1 = a.q.sortedQ[spos];
     const int nb = a.nblock;
     const double xf = 0.5 * fabs(a.kfac) * a.nx;
+    int64_t acc = 0;
     for (int sub = 0; sub < NSUB; ++sub) {
         const int seg = CY * NSUB + sub;
         int64_t kb, ke;
         ket_range<RT>(a.q, seg, spos, kb, ke);
         if (ke <= kb) continue;
+        const int64_t wk = ket_work<CX, CY>(sub) * st.nbp;
+        int64_t k0, k1;
+        window_kets(w0, w1, acc, wk, ke - kb, k0, k1);
+        acc += (ke - kb) * wk;
+        if (k1 <= k0) continue;
         auto keep = [&](int pos) {
             const int P2 = a.q.sorted[pos];
             const int C = a.q.pv.pa_blk[P2], Dd = a.q.pv.pb_blk[P2];
@@ -562,19 +570,21 @@ __device__ __forceinline__ void grad_ket_class(const GradArgs& a, const BraStage
             grad_column<CX, CY, RT, RS>(a, st, a.q.sorted[pos], q1 * a.q.sortedQ[pos], cd / Q::ND, cd % Q::ND, kg,
                                         gab, gsh, Rs);
         };
-        const int j0 = a.q.seg_start[seg] + static_cast<int>(kb);
+        const int j0 = a.q.seg_start[seg] + static_cast<int>(kb + k0);
         if constexpr (RS) {
-            ket_items_r<Q::L + 1>(Q::NCD * nkg, j0, ke - kb, kq, rot, st, a.q, Rbuf, keep, work);
+            ket_items_r<Q::L + 1>(Q::NCD * nkg, j0, k1 - k0, kq, rot, st, a.q, Rbuf, keep, work);
         } else {
-            ket_items(Q::NCD * nkg, j0, ke - kb, kq, rot, keep,
+            ket_items(Q::NCD * nkg, j0, k1 - k0, kq, rot, keep,
                       [&](int pos, int r) { work(pos, r, static_cast<const RT*>(nullptr)); });
         }
     }
 }
 
-// One kernel per (bra class, ket class): CTA per bra pair of class CX, items
-// over the ket segments of class CY. Dynamic shared memory: gradient
-// accumulator [natm][3], bra E tables (+1).
+// One kernel per (bra class, ket class), persistent: a CTA runs chunks
+// (bra pair of class CX, window of its ket pairs of class CY) of the
+// launch's work plan until it is used up. Dynamic shared memory: gradient
+// accumulator [natm][3] (one per CTA, flushed at the end), staged R, bra E
+// tables (+1).
 // RT = double: the FP64 quartets; RT = float: the FP32 quartets of the
 // mixed-precision path (accumulated in FP64).
 #ifndef AIMD_GRAD_MINB
@@ -589,35 +599,37 @@ __global__ void __launch_bounds__(128, AIMD_GRAD_MINB) grad2e_bra_kernel(GradArg
     RT* Esm = Rbuf + a.rbuf;
     __shared__ BraStageT<RT> st;
     __shared__ KetQueueR kq;
-    __shared__ int any;
-    const int spos = a.q.cls_start[CX] + blockIdx.x;
-    if (threadIdx.x == 0) {
-        load_stage(a.q, a.q.sorted[spos], st, Esm);
-        st.D = st.E + (size_t)st.nbp * BraE<Q0::LA, Q0::LB, 1>::SIZE;
-        int64_t tot = 0;
-        for (int sub = 0; sub < NSUB; ++sub) {
-            int64_t kb, ke;
-            ket_range<RT>(a.q, CY * NSUB + sub, spos, kb, ke);
-            tot += ke > kb ? ke - kb : 0;
-        }
-        any = tot > 0;
-    }
-    __syncthreads();
-    if (!any) return;
+    __shared__ int sh[2];
+    const int nbra = a.q.cls_start[CX + 1] - a.q.cls_start[CX];
+    const int total = a.plan.off[nbra];
     for (int i = threadIdx.x; i < 3 * a.natm; i += blockDim.x) gsh[i] = 0;
-    stage_bra_e<Q0::LA, Q0::LB, 1>(st);
-    __syncthreads();
-    stage_bra_d<Q0::LA, Q0::LB>(st);
-    __syncthreads();
-    double gab[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    int rot = 0;
-    grad_ket_class<CX, CY, RT>(a, st, spos, gab, gsh, kq, rot, Rbuf);
+    for (;;) {
+        int c, b;
+        next_chunk(a.plan, nbra, sh, c, b);                     // (its barrier also orders the zeroing)
+        if (c >= total) break;                                  // uniform: c is shared
+        const int spos = a.q.cls_start[CX] + b;
+        const int nch = a.plan.off[b + 1] - a.plan.off[b], j = c - a.plan.off[b];
+        const int64_t W = bra_work<CX, CY, RT>(a.q, spos);
+        if (threadIdx.x == 0) {
+            load_stage(a.q, a.q.sorted[spos], st, Esm);
+            st.D = st.E + (size_t)st.nbp * BraE<Q0::LA, Q0::LB, 1>::SIZE;
+        }
+        __syncthreads();
+        stage_bra_e<Q0::LA, Q0::LB, 1>(st);
+        __syncthreads();
+        stage_bra_d<Q0::LA, Q0::LB>(st);
+        __syncthreads();
+        double gab[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        int rot = 0;
+        grad_ket_class<CX, CY, RT>(a, st, spos, gab, gsh, kq, rot, Rbuf, chunk_edge(W, j, nch),
+                                   chunk_edge(W, j + 1, nch));
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        if (gab[d] != 0.0) fadd(gsh + 3 * st.aA + d, gab[d], FIX_G);
-        if (gab[3 + d] != 0.0) fadd(gsh + 3 * st.aB + d, gab[3 + d], FIX_G);
+        for (int d = 0; d < 3; ++d) {
+            if (gab[d] != 0.0) fadd(gsh + 3 * st.aA + d, gab[d], FIX_G);
+            if (gab[3 + d] != 0.0) fadd(gsh + 3 * st.aB + d, gab[3 + d], FIX_G);
+        }
+        __syncthreads();
     }
-    __syncthreads();
     for (int i = threadIdx.x; i < 3 * a.natm; i += blockDim.x)
         if (gsh[i] != 0) atomicAdd(a.grad + i, gsh[i]);
 }

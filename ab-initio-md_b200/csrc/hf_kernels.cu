@@ -72,6 +72,8 @@ struct aimd_ctx {
     double* bmax;           // [nblock][nblock] max |D| per block pair
     double* dmax;           // [1] max over bmax
     double* jkfix;          // [1] fixed-point scale of the J/K accumulators
+    int* plan;              // work plans of the class kernels (LaunchEnv::plan_of)
+    int* plan_next;         // their chunk counters
     double* bmc;            // gradient: [nblock][nblock] max |Dc| and max over x of |Dx|
     double* bmx;
     cudaStream_t cls_stream[NCLS];
@@ -237,6 +239,8 @@ extern "C" int aimd_create(aimd_ctx** out, int natm, int nao, int nblock, const 
         CK(dalloc(&c->bmax, (size_t)nblock * nblock));
         CK(dalloc(&c->dmax, 1));
         CK(dalloc(&c->jkfix, 1));
+        CK(dalloc(&c->plan, (size_t)2 * NCLS * (np + NCLS)));
+        CK(dalloc(&c->plan_next, (size_t)2 * NCLS * NCLS));
         CK(dalloc(&c->bmc, (size_t)nblock * nblock));
         CK(dalloc(&c->bmx, (size_t)nblock * nblock));
         for (int cl = 0; cl < NCLS; ++cl) c->maxbp[cl] = 1;
@@ -263,7 +267,7 @@ extern "C" int aimd_destroy(aimd_ctx* c) {
                     c->sh_atom, c->sh_l, c->sh_ao, c->sh_p0, c->sh_np, c->sp_i, c->sp_j, c->sh_exp, c->sh_coef,
                     c->charges, c->pa, c->pb, c->npp, c->slot, c->rec, c->Q, c->by_class, c->idx_in,
                     c->tmp_idx, c->seg_id, c->seg_keys, c->seg_keys_out, c->seg_start, c->tmpQ, c->sortedQ,
-                    c->sorted, c->counts_jk, c->counts_g, c->counts_d, c->bmax, c->dmax, c->jkfix, c->bmc, c->bmx, c->counts_hi, c->counts_hi_d, c->cub_tmp, c->pos, c->jacc, c->kacc, c->gacc};
+                    c->sorted, c->counts_jk, c->counts_g, c->counts_d, c->bmax, c->dmax, c->jkfix, c->plan, c->plan_next, c->bmc, c->bmx, c->counts_hi, c->counts_hi_d, c->cub_tmp, c->pos, c->jacc, c->kacc, c->gacc};
     for (void* p : ptrs) cudaFree(p);
     for (int i = 0; i < NCLS; ++i) {
         if (c->cls_stream[i]) cudaStreamDestroy(c->cls_stream[i]);
@@ -484,7 +488,102 @@ LaunchEnv launch_env(aimd_ctx* c) {
     e.natm = c->natm;
     e.by_class = c->by_class;
     e.Q = c->Q;
+    e.nsm = c->nsm;
+    e.plan = c->plan;
+    e.plan_next = c->plan_next;
+    e.plan_stride = c->npair + NCLS;
     return e;
+}
+
+// Work plan of the (CX, CY, RT) launch (one CTA of PLAN_THREADS): per bra
+// of class CX its chunk count ceil(W / target), target = max(total W /
+// (8 x resident CTAs), PLAN_MIN_WORK), as an exclusive prefix in off[0 ..
+// nbra]; the launch's chunk counter is zeroed.
+constexpr int PLAN_THREADS = 1024;
+constexpr int64_t PLAN_MIN_WORK = 4096;
+
+template <typename T>
+__device__ T block_sum(T v, T* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int d = 16; d > 0; d >>= 1) v += __shfl_down_sync(0xffffffffu, v, d);
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    T t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    return t;
+}
+
+template <int CX, int CY, typename RT>
+__device__ void plan_launch(const QuartetArgs& q, int* off, int* next, int resident) {
+    __shared__ int64_t red[PLAN_THREADS / 32];
+    __shared__ int ired[PLAN_THREADS / 32];
+    const int nbra = q.cls_start[CX + 1] - q.cls_start[CX];
+    const int per = (nbra + PLAN_THREADS - 1) / PLAN_THREADS;
+    const int b0 = min(nbra, (int)threadIdx.x * per), b1 = min(nbra, b0 + per);
+    int64_t w = 0;
+    for (int b = b0; b < b1; ++b) w += bra_work<CX, CY, RT>(q, q.cls_start[CX] + b);
+    const int64_t W = block_sum(w, red);
+    int64_t target = W / (8 * (int64_t)resident);
+    if (target < PLAN_MIN_WORK) target = PLAN_MIN_WORK;
+    int cnt = 0;
+    for (int b = b0; b < b1; ++b) {
+        const int64_t wb = bra_work<CX, CY, RT>(q, q.cls_start[CX] + b);
+        off[b] = (int)((wb + target - 1) / target);
+        cnt += off[b];
+    }
+    // exclusive scan of the per-thread counts (threads in index order)
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int incl = cnt;
+    for (int d = 1; d < 32; d <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += v;
+    }
+    if (lane == 31) ired[warp] = incl;
+    __syncthreads();
+    int base = incl - cnt;
+    for (int w2 = 0; w2 < warp; ++w2) base += ired[w2];
+    for (int b = b0; b < b1; ++b) {
+        const int k = off[b];
+        off[b] = base;
+        base += k;
+    }
+    if (threadIdx.x == PLAN_THREADS - 1) {
+        off[nbra] = base;                               // the last thread ends at the total
+        *next = 0;
+    }
+}
+
+// one CTA per (bra class, ket class <= bra class, type): blockIdx.x = pair
+// index CX (CX + 1) / 2 + CY, blockIdx.y = type (0: FP64 ranges, 1: FP32)
+__global__ void __launch_bounds__(PLAN_THREADS) plan_kernel(QuartetArgs q, int* plan, int* plan_next, int stride,
+                                                            int resident) {
+    int cx = 0;
+    while ((cx + 1) * (cx + 2) / 2 <= (int)blockIdx.x) ++cx;
+    const int cy = blockIdx.x - cx * (cx + 1) / 2, rt = blockIdx.y;
+    int* off = plan + (size_t)(rt * NCLS + cy) * stride + q.cls_start[cx] + cx;
+    int* next = plan_next + (rt * NCLS + cx) * NCLS + cy;
+#define AIMD_PLAN(X, Y)                                                         \
+    if (cx == X && cy == Y) {                                                   \
+        if (rt == 0) plan_launch<X, Y, double>(q, off, next, resident);        \
+        else plan_launch<X, Y, float>(q, off, next, resident);                 \
+    }
+    AIMD_PLAN(0, 0)
+    AIMD_PLAN(1, 0) AIMD_PLAN(1, 1)
+    AIMD_PLAN(2, 0) AIMD_PLAN(2, 1) AIMD_PLAN(2, 2)
+    AIMD_PLAN(3, 0) AIMD_PLAN(3, 1) AIMD_PLAN(3, 2) AIMD_PLAN(3, 3)
+    AIMD_PLAN(4, 0) AIMD_PLAN(4, 1) AIMD_PLAN(4, 2) AIMD_PLAN(4, 3) AIMD_PLAN(4, 4)
+    AIMD_PLAN(5, 0) AIMD_PLAN(5, 1) AIMD_PLAN(5, 2) AIMD_PLAN(5, 3) AIMD_PLAN(5, 4) AIMD_PLAN(5, 5)
+#undef AIMD_PLAN
+}
+
+// Plans of every class launch of one call (mixed: the FP32 ones too), on st
+// before the class streams fork.
+void plan_launches(aimd_ctx* c, const QuartetArgs& q, bool mixed, cudaStream_t st) {
+    plan_kernel<<<dim3(NCLS * (NCLS + 1) / 2, mixed ? 2 : 1), PLAN_THREADS, 0, st>>>(q, c->plan, c->plan_next,
+                                                                                   c->npair + NCLS, 2 * c->nsm);
+    ++c->launches;
 }
 
 // all (CX, CY <= CX) gradient kernels of bra class CX, in order on one stream
@@ -677,6 +776,7 @@ extern "C" int aimd_jk(aimd_ctx* c, int nset, const double* D, double* J, double
         a.dthr = 0.0;
         a.rbuf = 0;
         a.kglobal = c->jk_global_rows;
+        plan_launches(c, a.q, mixed, st);
 #define AIMD_JK(X, S) first_error(launch_jk_c##X(e, a, S), mixed ? launch_jk32_c##X(e, a, S) : cudaSuccess)
 #define AIMD_NL(X) jk_launches(c, X, mixed)
         AIMD_EACH_CLASS_CONCURRENT(AIMD_JK, "aimd_jk", AIMD_NL);
@@ -752,6 +852,7 @@ extern "C" int aimd_jk_delta(aimd_ctx* c, int nset, const double* D, double* J, 
         a.dthr = dthr;
         a.rbuf = 0;
         a.kglobal = c->jk_global_rows;
+        plan_launches(c, a.q, mixed, st);
 #define AIMD_JK(X, S) first_error(launch_jk_c##X(e, a, S), mixed ? launch_jk32_c##X(e, a, S) : cudaSuccess)
 #define AIMD_NL(X) jk_launches(c, X, mixed)
         AIMD_EACH_CLASS_CONCURRENT(AIMD_JK, "aimd_jk_delta", AIMD_NL);
@@ -921,6 +1022,7 @@ extern "C" int aimd_grad2e(aimd_ctx* c, const double* Dc, int nx, const double* 
     a.bmc = c->bmc;
     a.bmx = c->bmx;
     a.nblock = c->nblock;
+    plan_launches(c, a.q, mixed, st);
     const LaunchEnv e = launch_env(c);
 #define AIMD_GRAD(X, S) launch_grad_class<X>(e, a, S)
 #define AIMD_NL(X) grad_launches(c, X, mixed)

@@ -20,7 +20,25 @@ struct LaunchEnv {
     int nao, natm;
     const int* by_class;     // pair indices grouped by class
     double* Q;
+    int nsm;                 // SMs of the device
+    // work plans of the class kernels: per (type, ket class) one [npair +
+    // NCLS] array holding the [nbra + 1] prefix of each bra class in turn;
+    // chunk counters per (type, bra class, ket class)
+    int* plan;
+    int* plan_next;
+    int plan_stride;
+    WorkPlan plan_of(int cx, int cy, int rt) const {
+        return WorkPlan{plan + (size_t)(rt * NCLS + cy) * plan_stride + cls_start[cx] + cx,
+                        plan_next + (rt * NCLS + cx) * NCLS + cy};
+    }
 };
+
+// CTAs of a persistent launch of `kernel`: as many as fit on the device.
+inline int persistent_grid(const void* kernel, int threads, size_t smem, int nsm) {
+    int per = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem) != cudaSuccess || per < 1) per = 1;
+    return per * nsm;
+}
 
 // Status: cudaSuccess, a CUDA error, or cudaErrorInvalidConfiguration when
 // the shared-memory request exceeds the per-CTA limit.
