@@ -39,7 +39,7 @@ cudaError_t AIMD_GRAD_NAME(const LaunchEnv& e, const GradArgs& a0, cudaStream_t 
     cudaError_t r = set_smem_limit(kernel, smem);
     if (r != cudaSuccess) return r;
     a.plan = e.plan_of(CX, CY, sizeof(RT) == sizeof(double) ? 0 : 1);
-    grad2e_bra_kernel<CX, CY, RT><<<persistent_grid(kernel, 128, smem, e.nsm), 128, smem, st>>>(a);
+    grad2e_bra_kernel<CX, CY, RT><<<persistent_grid(kernel, GRAD_THREADS, smem, e.nsm), GRAD_THREADS, smem, st>>>(a);
     return cudaGetLastError();
 }
 

@@ -41,6 +41,13 @@ struct QClass {
     // staged sub-chunks hold many items (measured: staging the classes with
     // many-primitive pairs starved the sub-chunks and was slower)
     static constexpr bool RSMEM = CX == 5 && CY >= 4;
+    // Column-blocked items: one item covers the NC columns (ic, id) of one
+    // id, so R_tuv of a primitive quartet is computed once for NC columns
+    // instead of once per column; for the s/p bra classes against p kets,
+    // where the NC x NROW x KG accumulators fit in registers
+    static constexpr bool CBLK = (CX == 1 || CX == 2) && CY >= 1;
+    static constexpr int NCB = CBLK ? NC : 1;       // columns per item
+    static constexpr int NITEM = NCD / NCB;         // column items per ket pair and contraction group
 };
 
 // Bra-side E tables with an extra +G in i and j (G = 1 for gradients).
@@ -131,6 +138,21 @@ __device__ __forceinline__ void select_row(const RT (&e)[IM + 1][JM + 1][T + 1],
             if (ii == i && jj == j)
 #pragma unroll
                 for (int t = 0; t <= T; ++t) out[t] = e[ii][jj][t];
+}
+
+// out[i][t] = e[i][j][t] for every i (runtime j), by predicated copies.
+template <int IM, int JM, int T, typename RT>
+__device__ __forceinline__ void select_j(const RT (&e)[IM + 1][JM + 1][T + 1], int j, RT (&out)[IM + 1][T + 1]) {
+#pragma unroll
+    for (int i = 0; i <= IM; ++i)
+#pragma unroll
+        for (int t = 0; t <= T; ++t) {
+            RT x = e[i][0][t];
+#pragma unroll
+            for (int jj = 1; jj <= JM; ++jj)
+                if (jj == j) x = e[i][jj][t];
+            out[i][t] = x;
+        }
 }
 
 // v[r][kk] = (row r | cd, contraction kk) of the quartet (staged bra pair,
@@ -378,6 +400,117 @@ __device__ __forceinline__ void eri_column_ket_outer(const BraStageT<RT>& st, co
     }
 }
 
+// v[ic][r][kk] = (row r | ic id, contraction kk) for the NC columns of one
+// id (column-blocked items): the ket-outer order with R_tuv of each
+// primitive quartet computed once and applied to every column; the ket E
+// rows of a column come from the per-primitive table at compile-time ic.
+template <int CX, int CY, typename RT>
+__device__ __forceinline__ void eri_cols_ket_outer(const BraStageT<RT>& st, const double* __restrict__ rk, int nkp,
+                                                   int id, int kg,
+                                                   RT (&v)[QClass<CX, CY>::NC][QClass<CX, CY>::NROW][QClass<CX, CY>::KG]) {
+    using Q = QClass<CX, CY>;
+    using BE = BraE<Q::LA, Q::LB, 0>;
+    constexpr int LA = Q::LA, LB = Q::LB, LC = Q::LC, LD = Q::LD, LAB = Q::LAB, LCD = Q::LCD, L = Q::L;
+    const int dx = cart_x(LD, id), dy = cart_y(LD, id), dz = cart_z(LD, id);
+    const RT fd = static_cast<RT>(cart_norm(dx, dy, dz));
+#pragma unroll
+    for (int c = 0; c < Q::NC; ++c)
+#pragma unroll
+        for (int r = 0; r < Q::NROW; ++r)
+#pragma unroll
+            for (int k = 0; k < Q::KG; ++k) v[c][r][k] = RT(0);
+    for (int ik = 0; ik < nkp; ++ik) {
+        const KetRecT<RT> k = load_ket<RT>(rk + (size_t)ik * PPW);
+        const RT q = k.a + k.b, oo2q = RT(0.5) / q, iq = RT(2) * oo2q;
+        // ket E of this id: ex[i][t] = E^{i, dx}_t for every i <= LC
+        RT ex[LC + 1][LCD + 1], ey[LC + 1][LCD + 1], ez[LC + 1][LCD + 1];
+        {
+            RT e[LC + 1][LD + 1][LCD + 1];
+            hermite_e<LC, LD>(k.QAx, k.QBx, oo2q, k.K, e);
+            select_j<LC, LD, LCD>(e, dx, ex);
+            hermite_e<LC, LD>(k.QAy, k.QBy, oo2q, RT(1), e);
+            select_j<LC, LD, LCD>(e, dy, ey);
+            hermite_e<LC, LD>(k.QAz, k.QBz, oo2q, RT(1), e);
+            select_j<LC, LD, LCD>(e, dz, ez);
+        }
+        RT ck[Q::KG];
+#pragma unroll
+        for (int i = 0; i < Q::KG; ++i) {
+            RT c = k.c[0];
+#pragma unroll
+            for (int j = 1; j < Q::KCD; ++j)
+                if (j == kg * Q::KG + i) c = k.c[j];
+            ck[i] = c * fd;
+        }
+        for (int ib = 0; ib < st.nbp; ++ib) {
+            const RT* sb = st.SB + ib * SBW;
+            const RT p = sb[0];
+            const RT rs = rsqrt_t(p + q);
+            const RT alpha = p * q * rs * rs;
+            const RT pref = RT(TWO_PI_2_5) * sb[1] * iq * rs;
+            RT R[nherm(L)];
+            hermite_r<L>(alpha, sb[2] - k.Qx, sb[3] - k.Qy, sb[4] - k.Qz, R);
+            const RT* E = st.E + (size_t)ib * BE::SIZE;
+#pragma unroll
+            for (int ic = 0; ic < Q::NC; ++ic) {
+                const int cx = cart_x(LC, ic), cy = cart_y(LC, ic), cz = cart_z(LC, ic);
+                const RT fc = static_cast<RT>(cart_norm(cx, cy, cz));
+                RT X[Q::NHB];
+#pragma unroll
+                for (int t = 0; t <= LAB; ++t)
+#pragma unroll
+                    for (int u = 0; u <= LAB - t; ++u)
+#pragma unroll
+                        for (int w = 0; w <= LAB - t - u; ++w) {
+                            RT s = RT(0);
+#pragma unroll
+                            for (int t2 = 0; t2 <= LCD; ++t2) {
+                                if (t2 > cx + dx) continue;
+#pragma unroll
+                                for (int u2 = 0; u2 <= LCD; ++u2) {
+                                    if (u2 > cy + dy) continue;
+                                    const RT exy = ((t2 + u2) & 1) ? -ex[cx][t2] * ey[cy][u2] : ex[cx][t2] * ey[cy][u2];
+#pragma unroll
+                                    for (int v2 = 0; v2 <= LCD; ++v2) {
+                                        if (v2 > cz + dz) continue;
+                                        const RT e = (v2 & 1) ? -exy * ez[cz][v2] : exy * ez[cz][v2];
+                                        s += e * R[hidx(t + t2, u + u2, w + v2)];
+                                    }
+                                }
+                            }
+                            X[hidx(t, u, w)] = pref * fc * s;
+                        }
+                // bra step of column ic
+#pragma unroll
+                for (int ia = 0; ia < Q::NA; ++ia) {
+                    const int ax = cart_x(LA, ia), ay = cart_y(LA, ia), az = cart_z(LA, ia);
+#pragma unroll
+                    for (int jb = 0; jb < Q::NB; ++jb) {
+                        const int bx = cart_x(LB, jb), by = cart_y(LB, jb), bz = cart_z(LB, jb);
+                        const RT fab = static_cast<RT>(cart_norm(ax, ay, az) * cart_norm(bx, by, bz));
+                        RT s = RT(0);
+#pragma unroll
+                        for (int t = 0; t <= ax + bx; ++t)
+#pragma unroll
+                            for (int u = 0; u <= ay + by; ++u) {
+                                const RT exy = E[BE::at(0, ax, bx, t)] * E[BE::at(1, ay, by, u)];
+#pragma unroll
+                                for (int w = 0; w <= az + bz; ++w) s += exy * E[BE::at(2, az, bz, w)] * X[hidx(t, u, w)];
+                            }
+                        s *= fab;
+#pragma unroll
+                        for (int kab = 0; kab < Q::KAB; ++kab) {
+                            const RT c = sb[8 + kab] * s;
+#pragma unroll
+                            for (int kk = 0; kk < Q::KG; ++kk) v[ic][kab * Q::NAB + ia * Q::NB + jb][kk] += c * ck[kk];
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
 // (row r | cd) of a quartet column: bra-outer order (the bra step once per
 // bra primitive) for the d-shell bra classes, whose pairs have few
 // primitives, and the ket-outer order for the others.
@@ -422,6 +555,16 @@ __device__ __forceinline__ void ket_range(const QuartetArgs& a, int seg, int spo
         e = a.counts_hi ? cnt : hi;
     }
 }
+
+// A thread's R_tuv in shared memory: element i at p[i * NT] (NT = threads
+// of the CTA, p = base + threadIdx.x), so that a warp's accesses to one
+// element fall in distinct banks. Frees the registers (or the local
+// memory) that a large R array takes through the contraction passes.
+template <typename RT, int NT>
+struct RColumn {
+    RT* p;
+    __device__ __forceinline__ RT& operator[](int i) const { return p[i * NT]; }
+};
 
 // ---------------------------------------------------------------- work plan
 // The class kernels are persistent: their CTAs take chunks of (bra pair,
@@ -883,14 +1026,7 @@ __device__ __forceinline__ void jk_ket_class(const JKArgs& a, const BraStageT<RT
         };
         // contraction groups that the segment's ket pairs actually carry
         const int nkg = seg_groups<Q::KG, Q::NKG>(sub);
-        auto work = [&](int pos, int r, const RT* Rs) {
-            const int kg = r % nkg, cd = r / nkg;
-            const int P2 = a.q.sorted[pos];
-            const int C = a.q.pv.pa_blk[P2], Dd = a.q.pv.pb_blk[P2];
-            const int ic = cd / Q::ND, id = cd % Q::ND;
-            RT v[Q::NROW][Q::KG];
-            eri_column<CX, CY, RT, Q::RSMEM>(st, a.q.pv.rec + a.q.pv.slot[P2] * PPW, a.q.pv.npp[P2], ic, id, kg, v,
-                                             Rs);
+        auto digest = [&](int P2, int C, int Dd, int ic, int id, int kg, const RT (&v)[Q::NROW][Q::KG]) {
             if constexpr (sizeof(RT) == sizeof(double)) {
                 jk_digest_column<CX, CY, NS, KGLOBAL>(a, st, P2, C, Dd, ic, id, kg, v, Jt, Ksm);
             } else {
@@ -903,11 +1039,28 @@ __device__ __forceinline__ void jk_ket_class(const JKArgs& a, const BraStageT<RT
                 jk_digest_column<CX, CY, NS, KGLOBAL>(a, st, P2, C, Dd, ic, id, kg, vd, Jt, Ksm);
             }
         };
+        auto work = [&](int pos, int r, const RT* Rs) {
+            const int kg = r % nkg, cd = r / nkg;
+            const int P2 = a.q.sorted[pos];
+            const int C = a.q.pv.pa_blk[P2], Dd = a.q.pv.pb_blk[P2];
+            const double* rk = a.q.pv.rec + a.q.pv.slot[P2] * PPW;
+            if constexpr (Q::CBLK) {
+                // item = the NC columns of one id
+                RT v[Q::NC][Q::NROW][Q::KG];
+                eri_cols_ket_outer<CX, CY, RT>(st, rk, a.q.pv.npp[P2], cd, kg, v);
+#pragma unroll
+                for (int ic = 0; ic < Q::NC; ++ic) digest(P2, C, Dd, ic, cd, kg, v[ic]);
+            } else {
+                RT v[Q::NROW][Q::KG];
+                eri_column<CX, CY, RT, Q::RSMEM>(st, rk, a.q.pv.npp[P2], cd / Q::ND, cd % Q::ND, kg, v, Rs);
+                digest(P2, C, Dd, cd / Q::ND, cd % Q::ND, kg, v);
+            }
+        };
         const int j0 = a.q.seg_start[seg] + static_cast<int>(kb + k0);
         if constexpr (Q::RSMEM) {
-            ket_items_r<Q::L>(Q::NCD * nkg, j0, k1 - k0, kq, rot, st, a.q, Rbuf, keep, work);
+            ket_items_r<Q::L>(Q::NITEM * nkg, j0, k1 - k0, kq, rot, st, a.q, Rbuf, keep, work);
         } else {
-            ket_items(Q::NCD * nkg, j0, k1 - k0, kq, rot, keep,
+            ket_items(Q::NITEM * nkg, j0, k1 - k0, kq, rot, keep,
                       [&](int pos, int r) { work(pos, r, static_cast<const RT*>(nullptr)); });
         }
     }

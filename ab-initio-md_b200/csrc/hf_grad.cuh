@@ -34,6 +34,22 @@ struct GradArgs {
     WorkPlan plan;          // chunks of the launch (set per launch)
 };
 
+constexpr int GRAD_THREADS = 128;
+
+// Two-stage items (R_tuv to L + 1 staged per primitive quartet) for the
+// gradient of class pair (CX, CY): the same classes as the J/K build.
+template <int CX, int CY>
+constexpr bool grad_rsmem() { return QClass<CX, CY>::RSMEM; }
+
+// The other classes keep each thread's R_tuv (to L + 1) in a shared-memory
+// column while its passes run, where the columns of the CTA take at most
+// 96 KB (two CTAs per SM): R to L + 1 is the largest array of the
+// gradient body, and in registers it pushes the body into local memory.
+template <int CX, int CY, typename RT>
+constexpr bool grad_rcol() {
+    return !grad_rsmem<CX, CY>() && nherm(QClass<CX, CY>::L + 1) * sizeof(RT) * GRAD_THREADS <= 96 * 1024;
+}
+
 // Bra derivative coefficients of one primitive pair, per direction d:
 //   k = 0 (centre A): 2a E^{i+1,j}_t - i E^{i-1,j}_t
 //   k = 1 (centre B): 2b E^{i,j+1}_t - j E^{i,j-1}_t
@@ -93,7 +109,8 @@ __device__ __forceinline__ void ket_deriv_rows(const RT (&e)[LC + 2][LD + 1][LC 
 template <int CX, int CY, typename RT, bool RS>
 __device__ __forceinline__ void grad_prims_hoisted(const BraStageT<RT>& st, const RT (&Gr)[QClass<CX, CY>::NROW][QClass<CX, CY>::KG],
                                                    const double* __restrict__ rk, int nkp, int ic, int id, int kg,
-                                                   RT (&dA)[3], RT (&dB)[3], RT (&dC)[3], const RT* __restrict__ Rs) {
+                                                   RT (&dA)[3], RT (&dB)[3], RT (&dC)[3], const RT* __restrict__ Rs,
+                                                   RT* Rcol) {
     using Q = QClass<CX, CY>;
     using BE = BraE<Q::LA, Q::LB, 1>;
     using BD = BraD<Q::LA, Q::LB>;
@@ -202,7 +219,8 @@ __device__ __forceinline__ void grad_prims_hoisted(const BraStageT<RT>& st, cons
 #pragma unroll
                             for (int kk = 0; kk < KG; ++kk) Xs[kk][hidx(t, u, w)] += sc[kk] * s;
                         }
-                // C pass: dC_d += sum_h Y_h sum_k (-1)^|k| dE^{cd}_{d,k} R_{h+k}
+                // C pass: dC_d += sum_h Y_h sum_k (-1)^|k| dE^{cd}_{d,k} R_{h+k},
+                // one direction d at a time (one accumulator live)
 #pragma unroll UH
                 for (int t = 0; t <= LAB; ++t)
 #pragma unroll UH
@@ -212,29 +230,27 @@ __device__ __forceinline__ void grad_prims_hoisted(const BraStageT<RT>& st, cons
                             RT yv = RT(0);
 #pragma unroll
                             for (int kk = 0; kk < KG; ++kk) yv += sc[kk] * Y[kk][hidx(t, u, w)];
-                            RT s0 = RT(0), s1 = RT(0), s2 = RT(0);
 #pragma unroll
-                            for (int t2 = 0; t2 <= LCD + 1; ++t2) {
-                                if (t2 > cx + dx + 1) continue;
+                            for (int d = 0; d < 3; ++d) {
+                                RT sd = RT(0);
 #pragma unroll
-                                for (int u2 = 0; u2 <= LCD + 1; ++u2) {
-                                    if (u2 > cy + dy + 1) continue;
+                                for (int t2 = 0; t2 <= LCD + 1; ++t2) {
+                                    if (t2 > cx + dx + (d == 0)) continue;
 #pragma unroll
-                                    for (int v2 = 0; v2 <= LCD + 1; ++v2) {
-                                        if (v2 > cz + dz + 1) continue;
-                                        const int over = (t2 > cx + dx) + (u2 > cy + dy) + (v2 > cz + dz);
-                                        if (over > 1) continue;
-                                        const RT r = ((t2 + u2 + v2) & 1) ? -R[hidx(t + t2, u + u2, w + v2)]
-                                                                              : R[hidx(t + t2, u + u2, w + v2)];
-                                        s0 += gx[t2] * ey[u2] * ez[v2] * r;
-                                        s1 += ex[t2] * gy[u2] * ez[v2] * r;
-                                        s2 += ex[t2] * ey[u2] * gz[v2] * r;
+                                    for (int u2 = 0; u2 <= LCD + 1; ++u2) {
+                                        if (u2 > cy + dy + (d == 1)) continue;
+                                        const RT fxy = (d == 0 ? gx[t2] : ex[t2]) * (d == 1 ? gy[u2] : ey[u2]);
+#pragma unroll
+                                        for (int v2 = 0; v2 <= LCD + 1; ++v2) {
+                                            if (v2 > cz + dz + (d == 2)) continue;
+                                            const RT r = ((t2 + u2 + v2) & 1) ? -R[hidx(t + t2, u + u2, w + v2)]
+                                                                                  : R[hidx(t + t2, u + u2, w + v2)];
+                                            sd += fxy * (d == 2 ? gz[v2] : ez[v2]) * r;
+                                        }
                                     }
                                 }
+                                dC[d] += yv * sd;
                             }
-                            dC[0] += yv * s0;
-                            dC[1] += yv * s1;
-                            dC[2] += yv * s2;
                         }
             };
             if constexpr (RS) {
@@ -245,8 +261,15 @@ __device__ __forceinline__ void grad_prims_hoisted(const BraStageT<RT>& st, cons
                 const RT alpha = p * q * rs * rs;
                 const RT pref = RT(TWO_PI_2_5) * sb[1] * (RT(2) * oo2q) * rs;
                 RT R[nherm(L)];
-                hermite_r<L>(alpha, sb[2] - k.Qx, sb[3] - k.Qy, sb[4] - k.Qz, R);
-                body(R, pref);
+                if constexpr (grad_rcol<CX, CY, RT>()) {
+                    hermite_r_scaled<L>(alpha, sb[2] - k.Qx, sb[3] - k.Qy, sb[4] - k.Qz, pref, R);
+#pragma unroll
+                    for (int i = 0; i < nherm(L); ++i) Rcol[i * GRAD_THREADS] = R[i];
+                    body(RColumn<RT, GRAD_THREADS>{Rcol}, RT(1));
+                } else {
+                    hermite_r<L>(alpha, sb[2] - k.Qx, sb[3] - k.Qy, sb[4] - k.Qz, R);
+                    body(R, pref);
+                }
             }
         }
         // bra pass (A, B) on the summed ket step, once per bra primitive
@@ -295,101 +318,28 @@ constexpr bool grad_hoist() {
     return CX >= 3 && sizeof(RT) * (Q::NROW * Q::KG + Q::KG * (Q::NHB + nherm(Q::LAB + 1))) <= 800;
 }
 
-// Gradient contribution of one column; adds A, B parts to gab and C, D
-// parts to the shared accumulator gsh[natm][3]. RS: pref * R_tuv (to L + 1)
-// of the ket pair's primitive quartets staged in Rs ([ik][ib][NH(L + 1)]).
-template <int CX, int CY, typename RT, bool RS = false>
-__device__ __forceinline__ void grad_column(const GradArgs& a, const BraStageT<RT>& st, int P2, double QQ, int ic,
-                                            int id, int kg, double (&gab)[6], facc* gsh,
-                                            const RT* __restrict__ Rs = nullptr) {
+// One primitive quartet (bra primitive sb/E/Db, ket primitive through its
+// column rows ex.. and derivative rows gx..) of one gradient column:
+// adds the A, B and C derivative parts. Everything is linear in pref * R.
+template <int CX, int CY, typename RT, typename RArr>
+__device__ __forceinline__ void grad_pq(const RT* sb, const RT* E, const RT* Db,
+                                        const RT (&Gr)[QClass<CX, CY>::NROW][QClass<CX, CY>::KG],
+                                        const RT (&ck)[QClass<CX, CY>::KG], int cx, int cy, int cz, int dx, int dy,
+                                        int dz, const RT (&ex)[QClass<CX, CY>::LCD + 2],
+                                        const RT (&ey)[QClass<CX, CY>::LCD + 2],
+                                        const RT (&ez)[QClass<CX, CY>::LCD + 2],
+                                        const RT (&gx)[QClass<CX, CY>::LCD + 2],
+                                        const RT (&gy)[QClass<CX, CY>::LCD + 2],
+                                        const RT (&gz)[QClass<CX, CY>::LCD + 2], const RArr& R, RT pref,
+                                        RT (&dA)[3], RT (&dB)[3], RT (&dC)[3]) {
     using Q = QClass<CX, CY>;
     using BE = BraE<Q::LA, Q::LB, 1>;
     using BD = BraD<Q::LA, Q::LB>;
-    constexpr int LA = Q::LA, LB = Q::LB, LC = Q::LC, LD = Q::LD, LAB = Q::LAB, LCD = Q::LCD, L = Q::L + 1;
+    constexpr int LA = Q::LA, LB = Q::LB, LAB = Q::LAB, LCD = Q::LCD, L = Q::L + 1;
     constexpr int NH1 = nherm(LAB + 1);
     constexpr int UH = L >= 5 ? 1 : 16;      // rolled outer Hermite loops for large classes
     constexpr int UW = L >= 7 ? 1 : 16;      // and the inner one for the largest (compile time)
-    const BlockView& bv = a.q.bv;
-    const int C = a.q.pv.pa_blk[P2], Dd = a.q.pv.pb_blk[P2];
-    const int aC = bv.atom[C], aD = bv.atom[Dd];
-    if (st.aA == st.aB && st.aB == aC && aC == aD) return;          // one-centre: invariant
-    const int nC = bv.ncon[C], nD = bv.ncon[Dd], oC = bv.ao[C], oD = bv.ao[Dd];
-    const int n = a.q.nao;
-    const size_t nn = (size_t)n * n;
-    const double deg = 0.5 * (st.A != st.B ? 2.0 : 1.0) * (C != Dd ? 2.0 : 1.0) * (st.P1 != P2 ? 2.0 : 1.0);
-    // Gamma column
-    double G[Q::NROW][Q::KG];
-    double gmax = 0.0;
-#pragma unroll
-    for (int kk = 0; kk < Q::KG; ++kk) {
-        const int kq = kg * Q::KG + kk;
-        const bool cv = kq < nC * nD;
-        const int kc = cv ? kq / nD : 0, kd = cv ? kq % nD : 0;
-        const size_t l = oC + kc * Q::NC + ic, sg = oD + kd * Q::ND + id;
-#pragma unroll
-        for (int r = 0; r < Q::NROW; ++r) {
-            const int kab = r / Q::NAB, ab = r % Q::NAB, ka = kab / st.nB, kb = kab % st.nB;
-            double val = 0.0;
-            if (cv && kab < st.nA * st.nB) {
-                const size_t m = st.oA + ka * Q::NA + ab / Q::NB, nb_ = st.oB + kb * Q::NB + ab % Q::NB;
-                val = __ldg(a.Dc + m * n + nb_) * __ldg(a.Dc + l * n + sg);
-                for (int x = 0; x < a.nx; ++x) {
-                    const double* X = a.Dx + x * nn;
-                    val -= 0.5 * a.kfac * (__ldg(X + m * n + l) * __ldg(X + nb_ * n + sg) +
-                                           __ldg(X + m * n + sg) * __ldg(X + nb_ * n + l));
-                }
-                val *= deg;
-            }
-            G[r][kk] = val;
-            gmax = fmax(gmax, fabs(val));
-        }
-    }
-    if (QQ == 0.0 || QQ * gmax < a.thr) return;
-    // the Gamma column in the arithmetic type of the quartet
-    RT Gr[Q::NROW][Q::KG];
-#pragma unroll
-    for (int r = 0; r < Q::NROW; ++r)
-#pragma unroll
-        for (int kk = 0; kk < Q::KG; ++kk) Gr[r][kk] = static_cast<RT>(G[r][kk]);
-    RT dA[3] = {0.0, 0.0, 0.0}, dB[3] = {0.0, 0.0, 0.0}, dC[3] = {0.0, 0.0, 0.0};
-    if constexpr (grad_hoist<CX, CY, RT>()) {
-        grad_prims_hoisted<CX, CY, RT, RS>(st, Gr, a.q.pv.rec + a.q.pv.slot[P2] * PPW, a.q.pv.npp[P2], ic, id, kg,
-                                           dA, dB, dC, Rs);
-    } else {
-    const int cx = cart_x(LC, ic), cy = cart_y(LC, ic), cz = cart_z(LC, ic);
-    const int dx = cart_x(LD, id), dy = cart_y(LD, id), dz = cart_z(LD, id);
-    const RT fcd = cart_norm(cx, cy, cz) * cart_norm(dx, dy, dz);
-    const double* rk = a.q.pv.rec + a.q.pv.slot[P2] * PPW;
-    const int nkp = a.q.pv.npp[P2];
-    for (int ik = 0; ik < nkp; ++ik) {
-        const KetRecT<RT> k = load_ket<RT>(rk + (size_t)ik * PPW);
-        const RT ec = k.a, q = ec + k.b, oo2q = RT(0.5) / q, iq = RT(2) * oo2q;
-        // ket E for this column, and d/dC_d of it (one extra in direction d)
-        RT ex[LCD + 2], ey[LCD + 2], ez[LCD + 2], gx[LCD + 2], gy[LCD + 2], gz[LCD + 2];
-        {
-            RT e[LC + 2][LD + 1][LCD + 2];
-            hermite_e<LC + 1, LD>(k.QAx, k.QBx, oo2q, k.K, e);
-            ket_deriv_rows<LC, LD>(e, cx, dx, ec, ex, gx);
-            hermite_e<LC + 1, LD>(k.QAy, k.QBy, oo2q, RT(1), e);
-            ket_deriv_rows<LC, LD>(e, cy, dy, ec, ey, gy);
-            hermite_e<LC + 1, LD>(k.QAz, k.QBz, oo2q, RT(1), e);
-            ket_deriv_rows<LC, LD>(e, cz, dz, ec, ez, gz);
-        }
-        RT ck[Q::KG];
-#pragma unroll
-        for (int i = 0; i < Q::KG; ++i) {
-            RT c = k.c[0];
-#pragma unroll
-            for (int j = 1; j < Q::KCD; ++j)
-                if (j == kg * Q::KG + i) c = k.c[j];
-            ck[i] = c * fcd;
-        }
-        for (int ib = 0; ib < st.nbp; ++ib) {
-            const RT* sb = st.SB + ib * SBW;
-            const RT* E = st.E + (size_t)ib * BE::SIZE;
-            const RT* Db = st.D + (size_t)ib * BD::SIZE;
-            // everything below is linear in pref * R_tuv (R up to L + 1)
-            auto body = [&](const auto& R, RT pref) {
+
             // Gamma contracted with this bra primitive's coefficients and f_ab,
             // then summed over the ket contractions: gq[ab] = sum_kk gb[ab][kk] ck[kk]
             RT gq[Q::NAB];
@@ -475,30 +425,128 @@ __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStageT<R
 #pragma unroll UW
                     for (int w = 0; w <= LAB - t - u; ++w) {
                         const RT yv = Y[hidx(t, u, w)];
-                        RT s0 = 0.0, s1 = 0.0, s2 = 0.0;
+                        // one direction d at a time (one accumulator live)
 #pragma unroll
-                        for (int t2 = 0; t2 <= LCD + 1; ++t2) {
-                            if (t2 > cx + dx + 1) continue;
+                        for (int d = 0; d < 3; ++d) {
+                            RT sd = 0.0;
 #pragma unroll
-                            for (int u2 = 0; u2 <= LCD + 1; ++u2) {
-                                if (u2 > cy + dy + 1) continue;
+                            for (int t2 = 0; t2 <= LCD + 1; ++t2) {
+                                if (t2 > cx + dx + (d == 0)) continue;
 #pragma unroll
-                                for (int v2 = 0; v2 <= LCD + 1; ++v2) {
-                                    if (v2 > cz + dz + 1) continue;
-                                    const int over = (t2 > cx + dx) + (u2 > cy + dy) + (v2 > cz + dz);
-                                    if (over > 1) continue;
-                                    const RT r = ((t2 + u2 + v2) & 1) ? -R[hidx(t + t2, u + u2, w + v2)]
-                                                                          : R[hidx(t + t2, u + u2, w + v2)];
-                                    s0 += gx[t2] * ey[u2] * ez[v2] * r;
-                                    s1 += ex[t2] * gy[u2] * ez[v2] * r;
-                                    s2 += ex[t2] * ey[u2] * gz[v2] * r;
+                                for (int u2 = 0; u2 <= LCD + 1; ++u2) {
+                                    if (u2 > cy + dy + (d == 1)) continue;
+                                    const RT fxy = (d == 0 ? gx[t2] : ex[t2]) * (d == 1 ? gy[u2] : ey[u2]);
+#pragma unroll
+                                    for (int v2 = 0; v2 <= LCD + 1; ++v2) {
+                                        if (v2 > cz + dz + (d == 2)) continue;
+                                        const RT r = ((t2 + u2 + v2) & 1) ? -R[hidx(t + t2, u + u2, w + v2)]
+                                                                              : R[hidx(t + t2, u + u2, w + v2)];
+                                        sd += fxy * (d == 2 ? gz[v2] : ez[v2]) * r;
+                                    }
                                 }
                             }
+                            dC[d] += yv * sd;
                         }
-                        dC[0] += yv * s0;
-                        dC[1] += yv * s1;
-                        dC[2] += yv * s2;
                     }
+}
+
+// Gradient contribution of one column; adds A, B parts to gab and C, D
+// parts to the shared accumulator gsh[natm][3]. RS: pref * R_tuv (to L + 1)
+// of the ket pair's primitive quartets staged in Rs ([ik][ib][NH(L + 1)]).
+template <int CX, int CY, typename RT, bool RS = false>
+__device__ __forceinline__ void grad_column(const GradArgs& a, const BraStageT<RT>& st, int P2, double QQ, int ic,
+                                            int id, int kg, double (&gab)[6], facc* gsh,
+                                            const RT* __restrict__ Rs, RT* Rcol) {
+    using Q = QClass<CX, CY>;
+    using BE = BraE<Q::LA, Q::LB, 1>;
+    using BD = BraD<Q::LA, Q::LB>;
+    constexpr int LA = Q::LA, LB = Q::LB, LC = Q::LC, LD = Q::LD, LAB = Q::LAB, LCD = Q::LCD, L = Q::L + 1;
+    constexpr int NH1 = nherm(LAB + 1);
+    constexpr int UH = L >= 5 ? 1 : 16;      // rolled outer Hermite loops for large classes
+    constexpr int UW = L >= 7 ? 1 : 16;      // and the inner one for the largest (compile time)
+    const BlockView& bv = a.q.bv;
+    const int C = a.q.pv.pa_blk[P2], Dd = a.q.pv.pb_blk[P2];
+    const int aC = bv.atom[C], aD = bv.atom[Dd];
+    if (st.aA == st.aB && st.aB == aC && aC == aD) return;          // one-centre: invariant
+    const int nC = bv.ncon[C], nD = bv.ncon[Dd], oC = bv.ao[C], oD = bv.ao[Dd];
+    const int n = a.q.nao;
+    const size_t nn = (size_t)n * n;
+    const double deg = 0.5 * (st.A != st.B ? 2.0 : 1.0) * (C != Dd ? 2.0 : 1.0) * (st.P1 != P2 ? 2.0 : 1.0);
+    // Gamma column
+    double G[Q::NROW][Q::KG];
+    double gmax = 0.0;
+#pragma unroll
+    for (int kk = 0; kk < Q::KG; ++kk) {
+        const int kq = kg * Q::KG + kk;
+        const bool cv = kq < nC * nD;
+        const int kc = cv ? kq / nD : 0, kd = cv ? kq % nD : 0;
+        const size_t l = oC + kc * Q::NC + ic, sg = oD + kd * Q::ND + id;
+#pragma unroll
+        for (int r = 0; r < Q::NROW; ++r) {
+            const int kab = r / Q::NAB, ab = r % Q::NAB, ka = kab / st.nB, kb = kab % st.nB;
+            double val = 0.0;
+            if (cv && kab < st.nA * st.nB) {
+                const size_t m = st.oA + ka * Q::NA + ab / Q::NB, nb_ = st.oB + kb * Q::NB + ab % Q::NB;
+                val = __ldg(a.Dc + m * n + nb_) * __ldg(a.Dc + l * n + sg);
+                for (int x = 0; x < a.nx; ++x) {
+                    const double* X = a.Dx + x * nn;
+                    val -= 0.5 * a.kfac * (__ldg(X + m * n + l) * __ldg(X + nb_ * n + sg) +
+                                           __ldg(X + m * n + sg) * __ldg(X + nb_ * n + l));
+                }
+                val *= deg;
+            }
+            G[r][kk] = val;
+            gmax = fmax(gmax, fabs(val));
+        }
+    }
+    if (QQ == 0.0 || QQ * gmax < a.thr) return;
+    // the Gamma column in the arithmetic type of the quartet
+    RT Gr[Q::NROW][Q::KG];
+#pragma unroll
+    for (int r = 0; r < Q::NROW; ++r)
+#pragma unroll
+        for (int kk = 0; kk < Q::KG; ++kk) Gr[r][kk] = static_cast<RT>(G[r][kk]);
+    RT dA[3] = {0.0, 0.0, 0.0}, dB[3] = {0.0, 0.0, 0.0}, dC[3] = {0.0, 0.0, 0.0};
+    if constexpr (grad_hoist<CX, CY, RT>()) {
+        grad_prims_hoisted<CX, CY, RT, RS>(st, Gr, a.q.pv.rec + a.q.pv.slot[P2] * PPW, a.q.pv.npp[P2], ic, id, kg,
+                                           dA, dB, dC, Rs, Rcol);
+    } else {
+    const int cx = cart_x(LC, ic), cy = cart_y(LC, ic), cz = cart_z(LC, ic);
+    const int dx = cart_x(LD, id), dy = cart_y(LD, id), dz = cart_z(LD, id);
+    const RT fcd = cart_norm(cx, cy, cz) * cart_norm(dx, dy, dz);
+    const double* rk = a.q.pv.rec + a.q.pv.slot[P2] * PPW;
+    const int nkp = a.q.pv.npp[P2];
+    for (int ik = 0; ik < nkp; ++ik) {
+        const KetRecT<RT> k = load_ket<RT>(rk + (size_t)ik * PPW);
+        const RT ec = k.a, q = ec + k.b, oo2q = RT(0.5) / q, iq = RT(2) * oo2q;
+        // ket E for this column, and d/dC_d of it (one extra in direction d)
+        RT ex[LCD + 2], ey[LCD + 2], ez[LCD + 2], gx[LCD + 2], gy[LCD + 2], gz[LCD + 2];
+        {
+            RT e[LC + 2][LD + 1][LCD + 2];
+            hermite_e<LC + 1, LD>(k.QAx, k.QBx, oo2q, k.K, e);
+            ket_deriv_rows<LC, LD>(e, cx, dx, ec, ex, gx);
+            hermite_e<LC + 1, LD>(k.QAy, k.QBy, oo2q, RT(1), e);
+            ket_deriv_rows<LC, LD>(e, cy, dy, ec, ey, gy);
+            hermite_e<LC + 1, LD>(k.QAz, k.QBz, oo2q, RT(1), e);
+            ket_deriv_rows<LC, LD>(e, cz, dz, ec, ez, gz);
+        }
+        RT ck[Q::KG];
+#pragma unroll
+        for (int i = 0; i < Q::KG; ++i) {
+            RT c = k.c[0];
+#pragma unroll
+            for (int j = 1; j < Q::KCD; ++j)
+                if (j == kg * Q::KG + i) c = k.c[j];
+            ck[i] = c * fcd;
+        }
+        for (int ib = 0; ib < st.nbp; ++ib) {
+            const RT* sb = st.SB + ib * SBW;
+            const RT* E = st.E + (size_t)ib * BE::SIZE;
+            const RT* Db = st.D + (size_t)ib * BD::SIZE;
+            // everything below is linear in pref * R_tuv (R up to L + 1)
+            auto body = [&](const auto& R, RT pref) {
+                grad_pq<CX, CY, RT>(sb, E, Db, Gr, ck, cx, cy, cz, dx, dy, dz, ex, ey, ez, gx, gy, gz, R, pref, dA, dB,
+                                    dC);
             };
             if constexpr (RS) {
                 body(Rs + (size_t)(ik * st.nbp + ib) * nherm(L), RT(1));
@@ -508,8 +556,15 @@ __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStageT<R
                 const RT alpha = p * q * rs * rs;
                 const RT pref = RT(TWO_PI_2_5) * sb[1] * iq * rs;
                 RT R[nherm(L)];
-                hermite_r<L>(alpha, sb[2] - k.Qx, sb[3] - k.Qy, sb[4] - k.Qz, R);
-                body(R, pref);
+                if constexpr (grad_rcol<CX, CY, RT>()) {
+                    hermite_r_scaled<L>(alpha, sb[2] - k.Qx, sb[3] - k.Qy, sb[4] - k.Qz, pref, R);
+#pragma unroll
+                    for (int i = 0; i < nherm(L); ++i) Rcol[i * GRAD_THREADS] = R[i];
+                    body(RColumn<RT, GRAD_THREADS>{Rcol}, RT(1));
+                } else {
+                    hermite_r<L>(alpha, sb[2] - k.Qx, sb[3] - k.Qy, sb[4] - k.Qz, R);
+                    body(R, pref);
+                }
             }
         }
     }
@@ -528,10 +583,6 @@ __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStageT<R
 // block quartet, deg [|Dc|_AB |Dc|_CD + |k|/2 nx (|Dx|_AC |Dx|_BD +
 // |Dx|_AD |Dx|_BC)] >= max|Gamma|, can reach the threshold and the quartet
 // is not one-centre; the exact per-column test follows in grad_column.
-// Two-stage items (R_tuv to L + 1 staged per primitive quartet) for the
-// gradient of class pair (CX, CY): the same classes as the J/K build.
-template <int CX, int CY>
-constexpr bool grad_rsmem() { return QClass<CX, CY>::RSMEM; }
 
 template <int CX, int CY, typename RT>
 __device__ __forceinline__ void grad_ket_class(const GradArgs& a, const BraStageT<RT>& st, int spos, double (&gab)[6],
@@ -568,7 +619,7 @@ __device__ __forceinline__ void grad_ket_class(const GradArgs& a, const BraStage
         auto work = [&](int pos, int r, const RT* Rs) {
             const int kg = r % nkg, cd = r / nkg;
             grad_column<CX, CY, RT, RS>(a, st, a.q.sorted[pos], q1 * a.q.sortedQ[pos], cd / Q::ND, cd % Q::ND, kg,
-                                        gab, gsh, Rs);
+                                        gab, gsh, Rs, Rbuf + threadIdx.x);
         };
         const int j0 = a.q.seg_start[seg] + static_cast<int>(kb + k0);
         if constexpr (RS) {
@@ -591,7 +642,7 @@ __device__ __forceinline__ void grad_ket_class(const GradArgs& a, const BraStage
 #define AIMD_GRAD_MINB 1
 #endif
 template <int CX, int CY, typename RT>
-__global__ void __launch_bounds__(128, AIMD_GRAD_MINB) grad2e_bra_kernel(GradArgs a) {
+__global__ void __launch_bounds__(GRAD_THREADS, AIMD_GRAD_MINB) grad2e_bra_kernel(GradArgs a) {
     using Q0 = QClass<CX, 0>;
     extern __shared__ double smem[];
     facc* gsh = reinterpret_cast<facc*>(smem);
@@ -634,11 +685,13 @@ __global__ void __launch_bounds__(128, AIMD_GRAD_MINB) grad2e_bra_kernel(GradArg
         if (gsh[i] != 0) atomicAdd(a.grad + i, gsh[i]);
 }
 
-// Elements of the staged-R buffer of the (CX, CY) gradient kernel.
+// Elements of the staged-R buffer of the (CX, CY) gradient kernel (the
+// two-stage classes), or of its threads' R columns.
 template <int CX, int CY, typename RT>
 size_t grad_rbuf_elems(int max_bra_prims, int max_ket_prims) {
     if constexpr (grad_rsmem<CX, CY>())
         return rsmem_bytes<QClass<CX, CY>::L + 1, RT>(max_bra_prims, max_ket_prims) / sizeof(RT);
+    if constexpr (grad_rcol<CX, CY, RT>()) return (size_t)nherm(QClass<CX, CY>::L + 1) * GRAD_THREADS;
     return 0;
 }
 
