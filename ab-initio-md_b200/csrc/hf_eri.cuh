@@ -172,7 +172,7 @@ __device__ __forceinline__ void select_j(const RT (&e)[IM + 1][JM + 1][T + 1], i
 template <int CX, int CY, typename RT, bool RS = false>
 __device__ __forceinline__ void eri_column_bra_outer(const BraStageT<RT>& st, const double* __restrict__ rk, int nkp, int ic,
                                            int id, int kg, RT (&v)[QClass<CX, CY>::NROW][QClass<CX, CY>::KG],
-                                           const RT* __restrict__ Rs = nullptr) {
+                                           const RT* __restrict__ Rs, int ib0, int ib1) {
     using Q = QClass<CX, CY>;
     using BE = BraE<Q::LA, Q::LB, 0>;
     constexpr int LA = Q::LA, LB = Q::LB, LC = Q::LC, LD = Q::LD, LAB = Q::LAB, LCD = Q::LCD, L = Q::L;
@@ -185,7 +185,7 @@ __device__ __forceinline__ void eri_column_bra_outer(const BraStageT<RT>& st, co
     for (int r = 0; r < Q::NROW; ++r)
 #pragma unroll
         for (int k = 0; k < Q::KG; ++k) v[r][k] = RT(0);
-    for (int ib = 0; ib < st.nbp; ++ib) {
+    for (int ib = ib0; ib < ib1; ++ib) {
         const RT* sb = st.SB + ib * SBW;
         RT Xs[Q::KG][Q::NHB];
 #pragma unroll
@@ -300,7 +300,8 @@ __device__ __forceinline__ void eri_column_bra_outer(const BraStageT<RT>& st, co
 // the bra steps it saves.
 template <int CX, int CY, typename RT>
 __device__ __forceinline__ void eri_column_ket_outer(const BraStageT<RT>& st, const double* __restrict__ rk, int nkp,
-                                                     int ic, int id, int kg, RT (&v)[QClass<CX, CY>::NROW][QClass<CX, CY>::KG]) {
+                                                     int ic, int id, int kg, RT (&v)[QClass<CX, CY>::NROW][QClass<CX, CY>::KG],
+                                                     int ib0, int ib1) {
     using Q = QClass<CX, CY>;
     using BE = BraE<Q::LA, Q::LB, 0>;
     constexpr int LA = Q::LA, LB = Q::LB, LC = Q::LC, LD = Q::LD, LAB = Q::LAB, LCD = Q::LCD, L = Q::L;
@@ -336,7 +337,7 @@ __device__ __forceinline__ void eri_column_ket_outer(const BraStageT<RT>& st, co
                 if (j == kg * Q::KG + i) c = k.c[j];
             ck[i] = c * fcd;
         }
-        for (int ib = 0; ib < st.nbp; ++ib) {
+        for (int ib = ib0; ib < ib1; ++ib) {
             const RT* sb = st.SB + ib * SBW;
             const RT p = sb[0];
             const RT rs = rsqrt_t(p + q);
@@ -407,7 +408,8 @@ __device__ __forceinline__ void eri_column_ket_outer(const BraStageT<RT>& st, co
 template <int CX, int CY, typename RT>
 __device__ __forceinline__ void eri_cols_ket_outer(const BraStageT<RT>& st, const double* __restrict__ rk, int nkp,
                                                    int id, int kg,
-                                                   RT (&v)[QClass<CX, CY>::NC][QClass<CX, CY>::NROW][QClass<CX, CY>::KG]) {
+                                                   RT (&v)[QClass<CX, CY>::NC][QClass<CX, CY>::NROW][QClass<CX, CY>::KG],
+                                                   int ib0, int ib1) {
     using Q = QClass<CX, CY>;
     using BE = BraE<Q::LA, Q::LB, 0>;
     constexpr int LA = Q::LA, LB = Q::LB, LC = Q::LC, LD = Q::LD, LAB = Q::LAB, LCD = Q::LCD, L = Q::L;
@@ -442,7 +444,7 @@ __device__ __forceinline__ void eri_cols_ket_outer(const BraStageT<RT>& st, cons
                 if (j == kg * Q::KG + i) c = k.c[j];
             ck[i] = c * fd;
         }
-        for (int ib = 0; ib < st.nbp; ++ib) {
+        for (int ib = ib0; ib < ib1; ++ib) {
             const RT* sb = st.SB + ib * SBW;
             const RT p = sb[0];
             const RT rs = rsqrt_t(p + q);
@@ -517,9 +519,9 @@ __device__ __forceinline__ void eri_cols_ket_outer(const BraStageT<RT>& st, cons
 template <int CX, int CY, typename RT, bool RS = false>
 __device__ __forceinline__ void eri_column(const BraStageT<RT>& st, const double* __restrict__ rk, int nkp, int ic,
                                            int id, int kg, RT (&v)[QClass<CX, CY>::NROW][QClass<CX, CY>::KG],
-                                           const RT* __restrict__ Rs = nullptr) {
-    if constexpr (RS || CX >= 3) eri_column_bra_outer<CX, CY, RT, RS>(st, rk, nkp, ic, id, kg, v, Rs);
-    else eri_column_ket_outer<CX, CY, RT>(st, rk, nkp, ic, id, kg, v);
+                                           const RT* __restrict__ Rs, int ib0, int ib1) {
+    if constexpr (RS || CX >= 3) eri_column_bra_outer<CX, CY, RT, RS>(st, rk, nkp, ic, id, kg, v, Rs, ib0, ib1);
+    else eri_column_ket_outer<CX, CY, RT>(st, rk, nkp, ic, id, kg, v, ib0, ib1);
 }
 
 // Everything the quartet kernels share.
@@ -801,6 +803,17 @@ __device__ __forceinline__ int64_t ket_work(int sub) {
     return (int64_t)ket_prims2(sub / NCONB) * Q::NCD * seg_groups<Q::KG, Q::NKG>(sub);
 }
 
+// Bra-primitive splits of the column items of a ket segment: an item of a
+// pair of many primitive quartets would run them all in one thread while
+// the rest of the CTA waits at the next barrier, so such items are split
+// over ranges of the bra primitives (about ITEM_PQ quartets each; the
+// partial columns are linear in the quartets and are digested one by one).
+constexpr int ITEM_PQ = 32;
+__device__ __forceinline__ int bra_splits(int nbp, int sub) {
+    const int s = nbp * ket_prims2(sub / NCONB) / (2 * ITEM_PQ);
+    return s < 1 ? 1 : (s > nbp ? nbp : s);
+}
+
 struct KetQueue {
     int pos[KQ_CAP];
     int wcnt[32];           // per-warp counts of one compaction step
@@ -1039,28 +1052,32 @@ __device__ __forceinline__ void jk_ket_class(const JKArgs& a, const BraStageT<RT
                 jk_digest_column<CX, CY, NS, KGLOBAL>(a, st, P2, C, Dd, ic, id, kg, vd, Jt, Ksm);
             }
         };
+        // item r = (contraction group, bra-primitive split, column block)
+        const int nsp = bra_splits(st.nbp, sub);
         auto work = [&](int pos, int r, const RT* Rs) {
-            const int kg = r % nkg, cd = r / nkg;
+            const int kg = r % nkg, sp = (r / nkg) % nsp, cd = r / (nkg * nsp);
+            const int ib0 = st.nbp * sp / nsp, ib1 = st.nbp * (sp + 1) / nsp;
             const int P2 = a.q.sorted[pos];
             const int C = a.q.pv.pa_blk[P2], Dd = a.q.pv.pb_blk[P2];
             const double* rk = a.q.pv.rec + a.q.pv.slot[P2] * PPW;
             if constexpr (Q::CBLK) {
                 // item = the NC columns of one id
                 RT v[Q::NC][Q::NROW][Q::KG];
-                eri_cols_ket_outer<CX, CY, RT>(st, rk, a.q.pv.npp[P2], cd, kg, v);
+                eri_cols_ket_outer<CX, CY, RT>(st, rk, a.q.pv.npp[P2], cd, kg, v, ib0, ib1);
 #pragma unroll
                 for (int ic = 0; ic < Q::NC; ++ic) digest(P2, C, Dd, ic, cd, kg, v[ic]);
             } else {
                 RT v[Q::NROW][Q::KG];
-                eri_column<CX, CY, RT, Q::RSMEM>(st, rk, a.q.pv.npp[P2], cd / Q::ND, cd % Q::ND, kg, v, Rs);
+                eri_column<CX, CY, RT, Q::RSMEM>(st, rk, a.q.pv.npp[P2], cd / Q::ND, cd % Q::ND, kg, v, Rs, ib0,
+                                                 ib1);
                 digest(P2, C, Dd, cd / Q::ND, cd % Q::ND, kg, v);
             }
         };
         const int j0 = a.q.seg_start[seg] + static_cast<int>(kb + k0);
         if constexpr (Q::RSMEM) {
-            ket_items_r<Q::L>(Q::NITEM * nkg, j0, k1 - k0, kq, rot, st, a.q, Rbuf, keep, work);
+            ket_items_r<Q::L>(Q::NITEM * nkg * nsp, j0, k1 - k0, kq, rot, st, a.q, Rbuf, keep, work);
         } else {
-            ket_items(Q::NITEM * nkg, j0, k1 - k0, kq, rot, keep,
+            ket_items(Q::NITEM * nkg * nsp, j0, k1 - k0, kq, rot, keep,
                       [&](int pos, int r) { work(pos, r, static_cast<const RT*>(nullptr)); });
         }
     }
@@ -1192,7 +1209,8 @@ __global__ void __launch_bounds__(64) schwarz_kernel(QuartetArgs a, const int* p
     for (int cd = threadIdx.x; cd < Q::NCD; cd += blockDim.x) {
         static_assert(Q::KG == Q::KCD, "diagonal quartets keep all contraction combinations in one item");
         double v[Q::NROW][Q::KCD];
-        eri_column<CX, CX>(st, st.rec, st.nbp, cd / Q::ND, cd % Q::ND, 0, v);
+        eri_column<CX, CX>(st, st.rec, st.nbp, cd / Q::ND, cd % Q::ND, 0, v, static_cast<const double*>(nullptr), 0,
+                           st.nbp);
         double m = 0.0;
 #pragma unroll
         for (int ka = 0; ka < Q::KA; ++ka)

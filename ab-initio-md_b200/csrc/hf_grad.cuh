@@ -110,7 +110,7 @@ template <int CX, int CY, typename RT, bool RS>
 __device__ __forceinline__ void grad_prims_hoisted(const BraStageT<RT>& st, const RT (&Gr)[QClass<CX, CY>::NROW][QClass<CX, CY>::KG],
                                                    const double* __restrict__ rk, int nkp, int ic, int id, int kg,
                                                    RT (&dA)[3], RT (&dB)[3], RT (&dC)[3], const RT* __restrict__ Rs,
-                                                   RT* Rcol) {
+                                                   RT* Rcol, int ib0, int ib1) {
     using Q = QClass<CX, CY>;
     using BE = BraE<Q::LA, Q::LB, 1>;
     using BD = BraD<Q::LA, Q::LB>;
@@ -122,7 +122,7 @@ __device__ __forceinline__ void grad_prims_hoisted(const BraStageT<RT>& st, cons
     const int cx = cart_x(LC, ic), cy = cart_y(LC, ic), cz = cart_z(LC, ic);
     const int dx = cart_x(LD, id), dy = cart_y(LD, id), dz = cart_z(LD, id);
     const RT fcd = cart_norm(cx, cy, cz) * cart_norm(dx, dy, dz);
-    for (int ib = 0; ib < st.nbp; ++ib) {
+    for (int ib = ib0; ib < ib1; ++ib) {
         const RT* sb = st.SB + ib * SBW;
         const RT* E = st.E + (size_t)ib * BE::SIZE;
         const RT* Db = st.D + (size_t)ib * BD::SIZE;
@@ -219,39 +219,43 @@ __device__ __forceinline__ void grad_prims_hoisted(const BraStageT<RT>& st, cons
 #pragma unroll
                             for (int kk = 0; kk < KG; ++kk) Xs[kk][hidx(t, u, w)] += sc[kk] * s;
                         }
-                // C pass: dC_d += sum_h Y_h sum_k (-1)^|k| dE^{cd}_{d,k} R_{h+k},
-                // one direction d at a time (one accumulator live)
+                // C pass: dC_d += sum_k dE^{cd}_{d,k} Z_k with Z_k = (-1)^|k| sum_h Y_h R_{h+k},
+                // k over the ket box widened by one in at most one direction
+                // (the rows are zero beyond their box): Z is shared by the
+                // three directions
+#pragma unroll
+                for (int t2 = 0; t2 <= LCD + 1; ++t2) {
+                    if (t2 > cx + dx + 1) continue;
+#pragma unroll
+                    for (int u2 = 0; u2 <= LCD + 1; ++u2) {
+                        if (u2 > cy + dy + 1) continue;
+#pragma unroll
+                        for (int v2 = 0; v2 <= LCD + 1; ++v2) {
+                            if (v2 > cz + dz + 1) continue;
+                            if ((t2 > cx + dx) + (u2 > cy + dy) + (v2 > cz + dz) > 1) continue;
+                            RT z[KG];
+#pragma unroll
+                            for (int kk = 0; kk < KG; ++kk) z[kk] = RT(0);
 #pragma unroll UH
-                for (int t = 0; t <= LAB; ++t)
+                            for (int t = 0; t <= LAB; ++t)
 #pragma unroll UH
-                    for (int u = 0; u <= LAB - t; ++u)
+                                for (int u = 0; u <= LAB - t; ++u)
 #pragma unroll UW
-                        for (int w = 0; w <= LAB - t - u; ++w) {
-                            RT yv = RT(0);
+                                    for (int w = 0; w <= LAB - t - u; ++w) {
+                                        const RT r = R[hidx(t + t2, u + u2, w + v2)];
 #pragma unroll
-                            for (int kk = 0; kk < KG; ++kk) yv += sc[kk] * Y[kk][hidx(t, u, w)];
-#pragma unroll
-                            for (int d = 0; d < 3; ++d) {
-                                RT sd = RT(0);
-#pragma unroll
-                                for (int t2 = 0; t2 <= LCD + 1; ++t2) {
-                                    if (t2 > cx + dx + (d == 0)) continue;
-#pragma unroll
-                                    for (int u2 = 0; u2 <= LCD + 1; ++u2) {
-                                        if (u2 > cy + dy + (d == 1)) continue;
-                                        const RT fxy = (d == 0 ? gx[t2] : ex[t2]) * (d == 1 ? gy[u2] : ey[u2]);
-#pragma unroll
-                                        for (int v2 = 0; v2 <= LCD + 1; ++v2) {
-                                            if (v2 > cz + dz + (d == 2)) continue;
-                                            const RT r = ((t2 + u2 + v2) & 1) ? -R[hidx(t + t2, u + u2, w + v2)]
-                                                                                  : R[hidx(t + t2, u + u2, w + v2)];
-                                            sd += fxy * (d == 2 ? gz[v2] : ez[v2]) * r;
-                                        }
+                                        for (int kk = 0; kk < KG; ++kk) z[kk] += Y[kk][hidx(t, u, w)] * r;
                                     }
-                                }
-                                dC[d] += yv * sd;
-                            }
+                            RT zs = RT(0);
+#pragma unroll
+                            for (int kk = 0; kk < KG; ++kk) zs += sc[kk] * z[kk];
+                            if ((t2 + u2 + v2) & 1) zs = -zs;
+                            dC[0] += gx[t2] * ey[u2] * ez[v2] * zs;
+                            dC[1] += ex[t2] * gy[u2] * ez[v2] * zs;
+                            dC[2] += ex[t2] * ey[u2] * gz[v2] * zs;
                         }
+                    }
+                }
             };
             if constexpr (RS) {
                 body(Rs + (size_t)(ik * st.nbp + ib) * nherm(L), RT(1));
@@ -384,7 +388,9 @@ __device__ __forceinline__ void grad_pq(const RT* sb, const RT* E, const RT* Db,
                         Xb[hidx(t, u, w)] = s;
                     }
             // C pass: Y_h = sum_ab gq[ab] E^{ab}_h (h <= LAB), then
-            // dC_d += sum_h Y_h sum_k (-1)^|k| dE^{cd}_{d,k} R_{h+k}
+            // dC_d += sum_h Y_h sum_k (-1)^|k| dE^{cd}_{d,k} R_{h+k} (in this
+            // order the per-direction form spills less than the Z form of
+            // the hoisted order)
             RT Y[Q::NHB];
 #pragma unroll
             for (int h = 0; h < Q::NHB; ++h) Y[h] = 0.0;
@@ -456,7 +462,7 @@ __device__ __forceinline__ void grad_pq(const RT* sb, const RT* E, const RT* Db,
 template <int CX, int CY, typename RT, bool RS = false>
 __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStageT<RT>& st, int P2, double QQ, int ic,
                                             int id, int kg, double (&gab)[6], facc* gsh,
-                                            const RT* __restrict__ Rs, RT* Rcol) {
+                                            const RT* __restrict__ Rs, RT* Rcol, int ib0, int ib1) {
     using Q = QClass<CX, CY>;
     using BE = BraE<Q::LA, Q::LB, 1>;
     using BD = BraD<Q::LA, Q::LB>;
@@ -509,7 +515,7 @@ __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStageT<R
     RT dA[3] = {0.0, 0.0, 0.0}, dB[3] = {0.0, 0.0, 0.0}, dC[3] = {0.0, 0.0, 0.0};
     if constexpr (grad_hoist<CX, CY, RT>()) {
         grad_prims_hoisted<CX, CY, RT, RS>(st, Gr, a.q.pv.rec + a.q.pv.slot[P2] * PPW, a.q.pv.npp[P2], ic, id, kg,
-                                           dA, dB, dC, Rs, Rcol);
+                                           dA, dB, dC, Rs, Rcol, ib0, ib1);
     } else {
     const int cx = cart_x(LC, ic), cy = cart_y(LC, ic), cz = cart_z(LC, ic);
     const int dx = cart_x(LD, id), dy = cart_y(LD, id), dz = cart_z(LD, id);
@@ -539,7 +545,7 @@ __device__ __forceinline__ void grad_column(const GradArgs& a, const BraStageT<R
                 if (j == kg * Q::KG + i) c = k.c[j];
             ck[i] = c * fcd;
         }
-        for (int ib = 0; ib < st.nbp; ++ib) {
+        for (int ib = ib0; ib < ib1; ++ib) {
             const RT* sb = st.SB + ib * SBW;
             const RT* E = st.E + (size_t)ib * BE::SIZE;
             const RT* Db = st.D + (size_t)ib * BD::SIZE;
@@ -616,16 +622,19 @@ __device__ __forceinline__ void grad_ket_class(const GradArgs& a, const BraStage
             return q1 * a.q.sortedQ[pos] * deg * gb >= a.thr;
         };
         const int nkg = seg_groups<Q::KG, Q::NKG>(sub);
+        // item r = (contraction group, bra-primitive split, column)
+        const int nsp = bra_splits(st.nbp, sub);
         auto work = [&](int pos, int r, const RT* Rs) {
-            const int kg = r % nkg, cd = r / nkg;
+            const int kg = r % nkg, sp = (r / nkg) % nsp, cd = r / (nkg * nsp);
             grad_column<CX, CY, RT, RS>(a, st, a.q.sorted[pos], q1 * a.q.sortedQ[pos], cd / Q::ND, cd % Q::ND, kg,
-                                        gab, gsh, Rs, Rbuf + threadIdx.x);
+                                        gab, gsh, Rs, Rbuf + threadIdx.x, st.nbp * sp / nsp,
+                                        st.nbp * (sp + 1) / nsp);
         };
         const int j0 = a.q.seg_start[seg] + static_cast<int>(kb + k0);
         if constexpr (RS) {
-            ket_items_r<Q::L + 1>(Q::NCD * nkg, j0, k1 - k0, kq, rot, st, a.q, Rbuf, keep, work);
+            ket_items_r<Q::L + 1>(Q::NCD * nkg * nsp, j0, k1 - k0, kq, rot, st, a.q, Rbuf, keep, work);
         } else {
-            ket_items(Q::NCD * nkg, j0, k1 - k0, kq, rot, keep,
+            ket_items(Q::NCD * nkg * nsp, j0, k1 - k0, kq, rot, keep,
                       [&](int pos, int r) { work(pos, r, static_cast<const RT*>(nullptr)); });
         }
     }
