@@ -314,12 +314,15 @@ __device__ __forceinline__ void grad_prims_hoisted(const BraStageT<RT>& st, cons
 
 // The hoisted order for the d-shell bra classes, where its register
 // footprint (Gamma column, Y and the summed ket step per contraction group)
-// fits; the per-primitive-quartet order for the others.
+// fits (up to the 127 doubles of the dd bras, whose pairs have one bra
+// primitive, so the bra pass runs once per column instead of once per ket
+// primitive); the per-primitive-quartet order for the others (measured:
+// hoisting the s/p bras, whose pairs have many primitives, was no faster).
 template <int CX, int CY, typename RT>
 constexpr bool grad_hoist() {
     using Q = QClass<CX, CY>;
     // d-shell bras only (few bra primitives; see eri_column)
-    return CX >= 3 && sizeof(RT) * (Q::NROW * Q::KG + Q::KG * (Q::NHB + nherm(Q::LAB + 1))) <= 800;
+    return CX >= 3 && sizeof(RT) * (Q::NROW * Q::KG + Q::KG * (Q::NHB + nherm(Q::LAB + 1))) <= 1100;
 }
 
 // One primitive quartet (bra primitive sb/E/Db, ket primitive through its
