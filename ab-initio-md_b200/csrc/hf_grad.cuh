@@ -117,8 +117,8 @@ __device__ __forceinline__ void grad_prims_hoisted(const BraStageT<RT>& st, cons
     constexpr int LA = Q::LA, LB = Q::LB, LC = Q::LC, LD = Q::LD, LAB = Q::LAB, LCD = Q::LCD, L = Q::L + 1;
     constexpr int NH1 = nherm(LAB + 1);
     constexpr int KG = Q::KG;
-    constexpr int UH = L >= 5 ? 1 : 16;
-    constexpr int UW = L >= 7 ? 1 : 16;
+    constexpr int UH = L >= 4 ? 1 : 16;     // rolled Hermite loops: smaller code (instruction fetch)
+    constexpr int UW = L >= 5 ? 1 : 16;
     const int cx = cart_x(LC, ic), cy = cart_y(LC, ic), cz = cart_z(LC, ic);
     const int dx = cart_x(LD, id), dy = cart_y(LD, id), dz = cart_z(LD, id);
     const RT fcd = cart_norm(cx, cy, cz) * cart_norm(dx, dy, dz);
