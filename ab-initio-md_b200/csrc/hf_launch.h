@@ -72,14 +72,21 @@ constexpr size_t kSmemLimit = 227 * 1024;     // dynamic shared memory per CTA (
 
 // Allow `bytes` of dynamic shared memory for `kernel`. The default limit is
 // 48 KB for static plus dynamic shared memory together, so the opt-in is
-// needed whenever the sum passes it; the sum may not pass kSmemLimit.
+// needed whenever the sum passes it; the sum may not pass kSmemLimit. The
+// attribute is per kernel and process-wide, and contexts of different
+// bases run the same kernels from several host threads at once (batched
+// geometries), so it is always raised to the whole per-CTA limit, never
+// set to one launch's need: a smaller value set by one thread would make
+// another thread's larger launch fail.
 inline cudaError_t set_smem_limit(const void* kernel, size_t bytes) {
     cudaFuncAttributes fa;
     cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
     if (e != cudaSuccess) return e;
     if (bytes + fa.sharedSizeBytes > kSmemLimit) return cudaErrorInvalidConfiguration;
-    if (bytes + fa.sharedSizeBytes > 48 * 1024)
-        return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (bytes + fa.sharedSizeBytes > 48 * 1024 &&
+        (size_t)fa.maxDynamicSharedSizeBytes + fa.sharedSizeBytes < kSmemLimit)
+        return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(kSmemLimit - fa.sharedSizeBytes));
     return cudaSuccess;
 }
 
