@@ -32,6 +32,8 @@ SIGNATURES = {
     "aimd_schwarz": (_i, [_vp, _vp, _vp]),
     "aimd_pair_count": (_i, [_vp]),
     "aimd_set_fp32_cutoff": (_i, [_vp, _d]),
+    "aimd_set_launch_shape": (_i, [_vp, _i, _i]),
+    "aimd_get_launch_shape": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i)]),
     "aimd_jk": (_i, [_vp, _i, _vp, _vp, _vp, _d, _vp]),
     "aimd_jk_delta": (_i, [_vp, _i, _vp, _vp, _vp, _d, _d, _vp]),
     "aimd_eri_tensor": (_i, [_vp, _vp, _d, _vp]),

@@ -216,6 +216,65 @@ class Engine:
                                            ctypes.c_void_p(g.data_ptr()), _stream()), "aimd_onee_grad")
         return g
 
+    # ------------------------------------------------------------ launch shape
+    DEFAULT_SHAPES = ((8, 32), (4, 32), (16, 32), (8, 16), (8, 64))
+
+    @property
+    def launch_shape(self) -> tuple[int, int]:
+        """(work-plan chunks per resident CTA, primitive quartets per split column item)."""
+        c, q = ctypes.c_int(), ctypes.c_int()
+        _lib.check(self.lib.aimd_get_launch_shape(self.handle, ctypes.byref(c), ctypes.byref(q)),
+                   "aimd_get_launch_shape")
+        return int(c.value), int(q.value)
+
+    def set_launch_shape(self, chunks_per_cta: int, item_pq: int) -> None:
+        _lib.check(self.lib.aimd_set_launch_shape(self.handle, int(chunks_per_cta), int(item_pq)),
+                   "aimd_set_launch_shape")
+
+    def autotune(self, D: torch.Tensor, thr: float, grad: tuple | None = None, shapes=None,
+                 jk_weight: float = 10.0, reps: int = 2, fp32_cutoff: float = 0.0) -> dict:
+        """
+        Pick the launch shape of this context by timing, at the current
+        geometry: for every candidate (chunks per resident CTA, quartets per
+        split item) one warm J/K build of the densities D[nset, n, n] and,
+        if ``grad = (Dc, Dx, kfac, thr, gamma_bound)`` is given, one
+        two-electron gradient, timed with CUDA events on the current stream
+        (best of ``reps``); the score is jk_weight x J/K time + gradient
+        time (an MD step runs about ten Fock builds per gradient). Sets and
+        returns the fastest shape with every candidate's timings.
+        """
+        shapes = tuple(shapes or self.DEFAULT_SHAPES)
+        if not shapes:
+            raise ValueError("autotune: no candidate launch shapes")
+        start = self.launch_shape
+
+        def timed(fn) -> float:
+            best = float("inf")
+            for _ in range(reps):
+                s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                s.record()
+                fn()
+                e.record()
+                e.synchronize()
+                best = min(best, s.elapsed_time(e))
+            return best
+
+        results = []
+        try:
+            for shape in shapes:
+                self.set_launch_shape(*shape)
+                self.jk_acc(D, thr, fp32_cutoff)                  # warm-up at this shape
+                t_jk = timed(lambda: self.jk_acc(D, thr, fp32_cutoff))
+                t_g = timed(lambda: self.grad2e(*grad, fp32_cutoff=fp32_cutoff)) if grad is not None else 0.0
+                results.append({"shape": tuple(shape), "jk_ms": t_jk, "grad_ms": t_g,
+                                "score": jk_weight * t_jk + t_g})
+        except Exception:
+            self.set_launch_shape(*start)
+            raise
+        best = min(results, key=lambda r: r["score"])
+        self.set_launch_shape(*best["shape"])
+        return {"shape": best["shape"], "candidates": results}
+
     # ------------------------------------------------------------ inspection
     def quartet_counts(self, which: int = 0) -> np.ndarray:
         out = np.zeros(36, dtype=np.int64)

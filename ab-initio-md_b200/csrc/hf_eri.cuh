@@ -673,6 +673,7 @@ struct JKArgs {
     // launch when the per-CTA shared rows, NF x nao doubles, would not fit)
     int kglobal;
     WorkPlan plan;      // chunks of the launch (set per launch)
+    int item_pq;        // primitive quartets per split column item (launch shape)
 };
 
 // Digest one column (fixed ket component pair cd, all ket contractions kk)
@@ -806,11 +807,12 @@ __device__ __forceinline__ int64_t ket_work(int sub) {
 // Bra-primitive splits of the column items of a ket segment: an item of a
 // pair of many primitive quartets would run them all in one thread while
 // the rest of the CTA waits at the next barrier, so such items are split
-// over ranges of the bra primitives (about ITEM_PQ quartets each; the
-// partial columns are linear in the quartets and are digested one by one).
+// over ranges of the bra primitives (about item_pq quartets each, a launch
+// shape of the context, default ITEM_PQ; the partial columns are linear in
+// the quartets and are digested one by one).
 constexpr int ITEM_PQ = 32;
-__device__ __forceinline__ int bra_splits(int nbp, int sub) {
-    const int s = nbp * ket_prims2(sub / NCONB) / (2 * ITEM_PQ);
+__device__ __forceinline__ int bra_splits(int nbp, int sub, int item_pq) {
+    const int s = nbp * ket_prims2(sub / NCONB) / (2 * item_pq);
     return s < 1 ? 1 : (s > nbp ? nbp : s);
 }
 
@@ -1053,7 +1055,7 @@ __device__ __forceinline__ void jk_ket_class(const JKArgs& a, const BraStageT<RT
             }
         };
         // item r = (contraction group, bra-primitive split, column block)
-        const int nsp = bra_splits(st.nbp, sub);
+        const int nsp = bra_splits(st.nbp, sub, a.item_pq);
         auto work = [&](int pos, int r, const RT* Rs) {
             const int kg = r % nkg, sp = (r / nkg) % nsp, cd = r / (nkg * nsp);
             const int ib0 = st.nbp * sp / nsp, ib1 = st.nbp * (sp + 1) / nsp;

@@ -32,6 +32,7 @@ struct GradArgs {
     const double* bmx;      // [nblock][nblock] max over x of |Dx| per block pair (nx > 0)
     int nblock;
     WorkPlan plan;          // chunks of the launch (set per launch)
+    int item_pq;            // primitive quartets per split column item (launch shape)
 };
 
 constexpr int GRAD_THREADS = 128;
@@ -626,7 +627,7 @@ __device__ __forceinline__ void grad_ket_class(const GradArgs& a, const BraStage
         };
         const int nkg = seg_groups<Q::KG, Q::NKG>(sub);
         // item r = (contraction group, bra-primitive split, column)
-        const int nsp = bra_splits(st.nbp, sub);
+        const int nsp = bra_splits(st.nbp, sub, a.item_pq);
         auto work = [&](int pos, int r, const RT* Rs) {
             const int kg = r % nkg, sp = (r / nkg) % nsp, cd = r / (nkg * nsp);
             grad_column<CX, CY, RT, RS>(a, st, a.q.sorted[pos], q1 * a.q.sortedQ[pos], cd / Q::ND, cd % Q::ND, kg,

@@ -74,6 +74,10 @@ struct aimd_ctx {
     double* jkfix;          // [1] fixed-point scale of the J/K accumulators
     int* plan;              // work plans of the class kernels (LaunchEnv::plan_of)
     int* plan_next;         // their chunk counters
+    // launch shape (aimd_set_launch_shape): work-plan chunks per resident
+    // CTA, primitive quartets per split column item
+    int plan_chunks = 8;
+    int item_pq = ITEM_PQ;
     double* bmc;            // gradient: [nblock][nblock] max |Dc| and max over x of |Dx|
     double* bmx;
     cudaStream_t cls_stream[NCLS];
@@ -497,8 +501,9 @@ LaunchEnv launch_env(aimd_ctx* c) {
 
 // Work plan of the (CX, CY, RT) launch (one CTA of PLAN_THREADS): per bra
 // of class CX its chunk count ceil(W / target), target = max(total W /
-// (8 x resident CTAs), PLAN_MIN_WORK), as an exclusive prefix in off[0 ..
-// nbra]; the launch's chunk counter is zeroed.
+// parts, PLAN_MIN_WORK) with parts = chunks per resident CTA x resident
+// CTAs, as an exclusive prefix in off[0 .. nbra]; the launch's chunk
+// counter is zeroed.
 constexpr int PLAN_THREADS = 1024;
 constexpr int64_t PLAN_MIN_WORK = 4096;
 
@@ -515,7 +520,7 @@ __device__ T block_sum(T v, T* red) {
 }
 
 template <int CX, int CY, typename RT>
-__device__ void plan_launch(const QuartetArgs& q, int* off, int* next, int resident) {
+__device__ void plan_launch(const QuartetArgs& q, int* off, int* next, int parts) {
     __shared__ int64_t red[PLAN_THREADS / 32];
     __shared__ int ired[PLAN_THREADS / 32];
     const int nbra = q.cls_start[CX + 1] - q.cls_start[CX];
@@ -524,7 +529,7 @@ __device__ void plan_launch(const QuartetArgs& q, int* off, int* next, int resid
     int64_t w = 0;
     for (int b = b0; b < b1; ++b) w += bra_work<CX, CY, RT>(q, q.cls_start[CX] + b);
     const int64_t W = block_sum(w, red);
-    int64_t target = W / (8 * (int64_t)resident);
+    int64_t target = W / parts;
     if (target < PLAN_MIN_WORK) target = PLAN_MIN_WORK;
     int cnt = 0;
     for (int b = b0; b < b1; ++b) {
@@ -558,7 +563,7 @@ __device__ void plan_launch(const QuartetArgs& q, int* off, int* next, int resid
 // one CTA per (bra class, ket class <= bra class, type): blockIdx.x = pair
 // index CX (CX + 1) / 2 + CY, blockIdx.y = type (0: FP64 ranges, 1: FP32)
 __global__ void __launch_bounds__(PLAN_THREADS) plan_kernel(QuartetArgs q, int* plan, int* plan_next, int stride,
-                                                            int resident) {
+                                                            int parts) {
     int cx = 0;
     while ((cx + 1) * (cx + 2) / 2 <= (int)blockIdx.x) ++cx;
     const int cy = blockIdx.x - cx * (cx + 1) / 2, rt = blockIdx.y;
@@ -566,8 +571,8 @@ __global__ void __launch_bounds__(PLAN_THREADS) plan_kernel(QuartetArgs q, int* 
     int* next = plan_next + (rt * NCLS + cx) * NCLS + cy;
 #define AIMD_PLAN(X, Y)                                                         \
     if (cx == X && cy == Y) {                                                   \
-        if (rt == 0) plan_launch<X, Y, double>(q, off, next, resident);        \
-        else plan_launch<X, Y, float>(q, off, next, resident);                 \
+        if (rt == 0) plan_launch<X, Y, double>(q, off, next, parts);           \
+        else plan_launch<X, Y, float>(q, off, next, parts);                    \
     }
     AIMD_PLAN(0, 0)
     AIMD_PLAN(1, 0) AIMD_PLAN(1, 1)
@@ -582,7 +587,8 @@ __global__ void __launch_bounds__(PLAN_THREADS) plan_kernel(QuartetArgs q, int* 
 // before the class streams fork.
 void plan_launches(aimd_ctx* c, const QuartetArgs& q, bool mixed, cudaStream_t st) {
     plan_kernel<<<dim3(NCLS * (NCLS + 1) / 2, mixed ? 2 : 1), PLAN_THREADS, 0, st>>>(q, c->plan, c->plan_next,
-                                                                                   c->npair + NCLS, 2 * c->nsm);
+                                                                                   c->npair + NCLS,
+                                                                                   c->plan_chunks * 2 * c->nsm);
     ++c->launches;
 }
 
@@ -698,6 +704,24 @@ extern "C" int aimd_set_fp32_cutoff(aimd_ctx* c, double cutoff) {
     return AIMD_OK;
 }
 
+extern "C" int aimd_set_launch_shape(aimd_ctx* c, int chunks_per_cta, int item_pq) {
+    if (!c || chunks_per_cta < 1 || chunks_per_cta > 64 || item_pq < 4 || item_pq > 4096) {
+        snprintf(g_err, sizeof g_err,
+                 "aimd_set_launch_shape: chunks_per_cta must be in 1..64 and item_pq in 4..4096");
+        return AIMD_ERR_ARG;
+    }
+    c->plan_chunks = chunks_per_cta;
+    c->item_pq = item_pq;
+    return AIMD_OK;
+}
+
+extern "C" int aimd_get_launch_shape(aimd_ctx* c, int* chunks_per_cta, int* item_pq) {
+    if (!c || !chunks_per_cta || !item_pq) return AIMD_ERR_ARG;
+    *chunks_per_cta = c->plan_chunks;
+    *item_pq = c->item_pq;
+    return AIMD_OK;
+}
+
 extern "C" int aimd_set_geometry(aimd_ctx* c, const double* pos, void* stream) {
     if (!c || !pos) return AIMD_ERR_ARG;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -776,6 +800,7 @@ extern "C" int aimd_jk(aimd_ctx* c, int nset, const double* D, double* J, double
         a.dthr = 0.0;
         a.rbuf = 0;
         a.kglobal = c->jk_global_rows;
+        a.item_pq = c->item_pq;
         plan_launches(c, a.q, mixed, st);
 #define AIMD_JK(X, S) first_error(launch_jk_c##X(e, a, S), mixed ? launch_jk32_c##X(e, a, S) : cudaSuccess)
 #define AIMD_NL(X) jk_launches(c, X, mixed)
@@ -852,6 +877,7 @@ extern "C" int aimd_jk_delta(aimd_ctx* c, int nset, const double* D, double* J, 
         a.dthr = dthr;
         a.rbuf = 0;
         a.kglobal = c->jk_global_rows;
+        a.item_pq = c->item_pq;
         plan_launches(c, a.q, mixed, st);
 #define AIMD_JK(X, S) first_error(launch_jk_c##X(e, a, S), mixed ? launch_jk32_c##X(e, a, S) : cudaSuccess)
 #define AIMD_NL(X) jk_launches(c, X, mixed)
@@ -1022,6 +1048,7 @@ extern "C" int aimd_grad2e(aimd_ctx* c, const double* Dc, int nx, const double* 
     a.bmc = c->bmc;
     a.bmx = c->bmx;
     a.nblock = c->nblock;
+    a.item_pq = c->item_pq;
     plan_launches(c, a.q, mixed, st);
     const LaunchEnv e = launch_env(c);
 #define AIMD_GRAD(X, S) launch_grad_class<X>(e, a, S)

@@ -63,6 +63,17 @@ int aimd_pair_count(aimd_ctx *ctx);
  * of the mixed-precision path, applied to the Schwarz product Q1 Q2. */
 int aimd_set_fp32_cutoff(aimd_ctx *ctx, double cutoff);
 
+/* Launch shape of the context's J/K and gradient kernels (no counterpart
+ * in the reference, whose numba loops have no launch geometry): the work of
+ * each class launch is cut into about chunks_per_cta x (resident CTAs)
+ * chunks that the persistent CTAs take in turn (1..64, default 8), and a
+ * column item of a pair with many primitive quartets is split over bra
+ * primitives into items of about item_pq quartets (4..4096, default 32).
+ * Results change only by rounding; aimd_b200.engine.Engine.autotune picks
+ * the shape by timing. AIMD_ERR_ARG outside the ranges. */
+int aimd_set_launch_shape(aimd_ctx *ctx, int chunks_per_cta, int item_pq);
+int aimd_get_launch_shape(aimd_ctx *ctx, int *chunks_per_cta, int *item_pq);
+
 /* Integral-direct J/K for nset symmetric densities D[nset][nao][nao]
  * (device). Writes the un-symmetrised accumulators: the caller forms
  * J = J + J^T and K = K + K^T. Quartets with Q1 Q2 < thr are skipped.
