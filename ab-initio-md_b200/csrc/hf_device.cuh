@@ -130,7 +130,9 @@ __device__ __forceinline__ double boys_top(double x, double ex) {
         return ex * s;
     }
     const double sx = sqrt(x);
-    double f = 0.88622692545275801365 * erf(sx) / sx;      // sqrt(pi)/2 erf(sqrt x)/sqrt x
+    // sqrt(pi)/2 erf(sqrt x)/sqrt x; from x = 36 on erf(sqrt x) is 1 in double
+    // precision (erfc(6) = 2.2e-17, below half an ulp of 1)
+    double f = 0.88622692545275801365 * (x < 36.0 ? erf(sx) : 1.0) / sx;
     if (N > 0) {
         const double inv2x = 0.5 / x;
 #pragma unroll
